@@ -1,0 +1,586 @@
+// C-ABI of the B200 multifrontal LDL^T (declared in include/b200ldl.h).
+//
+// A handle owns: the host symbolic analysis, the device plan (assembly and
+// extend-add maps, level lists), and the device pools of the last
+// factorization. Errors are returned as status codes with a message kept on
+// the handle; nothing aborts.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/b200ldl.h"
+#include "ldl_internal.h"
+#include "symbolic.h"
+
+using namespace b200ldl;
+
+namespace {
+
+template <typename T>
+struct DevBuf {
+  T* ptr = nullptr;
+  size_t count = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    count = 0;
+  }
+  cudaError_t alloc(size_t n) {
+    release();
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&ptr, n * sizeof(T));
+    if (e == cudaSuccess) count = n;
+    else ptr = nullptr;
+    return e;
+  }
+  cudaError_t upload(const std::vector<T>& h) {
+    cudaError_t e = alloc(h.size());
+    if (e != cudaSuccess) return e;
+    if (!h.empty()) e = cudaMemcpy(ptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return e;
+  }
+};
+
+struct CudaError : std::runtime_error {
+  cudaError_t code;
+  CudaError(cudaError_t c, const char* what)
+      : std::runtime_error(std::string(what) + ": " + cudaGetErrorString(c)), code(c) {}
+};
+
+#define CK(call)                                        \
+  do {                                                  \
+    cudaError_t e__ = (call);                           \
+    if (e__ != cudaSuccess) throw CudaError(e__, #call); \
+  } while (0)
+
+}  // namespace
+
+struct b200ldl_handle {
+  int n = 0, nnz = 0;
+  int solver_type = B200LDL_LDL;
+  double ustab = 0.01, pivot_tol = 1e-14, delay_growth = 2.0;
+  int order = B200LDL_ORDER_NATURAL;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+
+  Symbolic sym;
+  bool uploaded = false;
+  // host copies of the plan (uploaded lazily on the first factorization so
+  // that the symbolic phase runs on machines without a GPU)
+  std::vector<int> hp_ns, hp_nc, hp_kid_ptr, hp_kids, hp_cmap, hp_scat_csr, hp_scat_row,
+      hp_scat_col, hp_level_nodes;
+  std::vector<int64_t> hp_scat_ptr;
+  int num_levels = 0;
+  std::vector<int> level_ptr;  // host copy
+  std::vector<int> h_ns, h_nc;
+
+  // device plan
+  DevBuf<int> d_ns, d_nc, d_var_ptr, d_node_to_var, d_cptr, d_contrib_rows, d_cmap,
+      d_kid_ptr, d_kids, d_scat_csr, d_scat_row, d_scat_col, d_level_nodes;
+  DevBuf<int64_t> d_scat_ptr;
+  DevPlan plan{};
+
+  // device state
+  DevBuf<int> d_f, d_fs, d_npiv, d_ndel, d_L_ld, d_cb_ld, d_ivars, d_err, d_inertia;
+  DevBuf<int64_t> d_fv_off, d_L_off, d_cb_off, d_u_off;
+  DevBuf<double> d_dpool, d_flops, d_upool, d_vals, d_diag, d_x;
+  DevBuf<unsigned long long> d_used;
+  unsigned long long icap = 0, dcap = 0;
+  DevState st{};
+
+  // results of the last factorization
+  bool factored = false;
+  int inertia[2] = {0, 0};
+  unsigned long long used[3] = {0, 0, 0};
+  double exec_flops = 0.0;
+  int fmax = 0;
+  double sum_delayed = 0.0;
+};
+
+namespace {
+
+int fail(b200ldl_t h, int code, const char* fmt, ...) {
+  if (h) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    h->last_error = buf;
+  }
+  return code;
+}
+
+// Build the static assembly / extend-add maps and the level lists.
+void build_plan(b200ldl_t h, const int* rowp, const int* cols) {
+  const Symbolic& s = h->sym;
+  const int n = s.n;
+  const int nn = s.num_nodes;
+  std::vector<int> ns(nn), nc(nn);
+  for (int k = 0; k < nn; k++) {
+    ns[k] = s.node_ptr[k + 1] - s.node_ptr[k];
+    nc[k] = s.contrib_ptr[k + 1] - s.contrib_ptr[k];
+  }
+  std::vector<int> kid_ptr(s.children_ptr.begin(), s.children_ptr.begin() + nn + 1);
+  std::vector<int> kids(s.children.begin(), s.children.begin() + kid_ptr[nn]);
+
+  // positions of the front variables of node k (own vars then contrib rows)
+  std::vector<int> where(n, -1);
+  auto mark = [&](int k, int sign) {
+    for (int j = 0; j < ns[k]; j++) where[s.node_to_var[s.node_ptr[k] + j]] = sign ? j : -1;
+    for (int t = 0; t < nc[k]; t++)
+      where[s.contrib_rows[s.contrib_ptr[k] + t]] = sign ? ns[k] + t : -1;
+  };
+
+  std::vector<int> cmap(s.contrib_rows.size(), -1);
+  std::vector<int64_t> scat_ptr(nn + 1, 0);
+  std::vector<int> scat_csr, scat_row, scat_col;
+  scat_csr.reserve(rowp[n]);
+  scat_row.reserve(rowp[n]);
+  scat_col.reserve(rowp[n]);
+  const int* ip = s.iperm.data();
+  for (int k = 0; k < nn; k++) {
+    mark(k, 1);
+    for (int j = 0; j < ns[k]; j++) {
+      const int var = s.node_to_var[s.node_ptr[k] + j];
+      const int pj = ip[var];
+      for (int e = rowp[var]; e < rowp[var + 1]; e++) {
+        const int i = cols[e];
+        if (ip[i] < pj) continue;
+        const int w = where[i];
+        if (w < 0) continue;
+        scat_csr.push_back(e);
+        scat_row.push_back(w);
+        scat_col.push_back(j);
+      }
+    }
+    scat_ptr[k + 1] = (int64_t)scat_csr.size();
+    // children's contribution rows -> positions in this front
+    for (int c = kid_ptr[k]; c < kid_ptr[k + 1]; c++) {
+      const int ch = kids[c];
+      for (int t = s.contrib_ptr[ch]; t < s.contrib_ptr[ch + 1]; t++) {
+        const int w = where[s.contrib_rows[t]];
+        if (w < 0) throw std::runtime_error("contribution row missing from the parent front");
+        cmap[t] = w;
+      }
+    }
+    mark(k, 0);
+  }
+  for (int k = 0; k < nn; k++) {
+    if (s.parent[k] < 0 && nc[k] > 0)
+      throw std::runtime_error("root supernode with contribution rows");
+  }
+
+  // levels: leaves 0, parent = 1 + max(children)
+  std::vector<int> level(nn, 0);
+  bool post = true;
+  for (int k = 0; k < nn; k++)
+    if (s.parent[k] >= 0 && s.parent[k] <= k) post = false;
+  if (post) {
+    for (int k = 0; k < nn; k++)
+      if (s.parent[k] >= 0) level[s.parent[k]] = std::max(level[s.parent[k]], level[k] + 1);
+  } else {
+    bool changed = true;
+    while (changed) {
+      changed = false;
+      for (int k = 0; k < nn; k++) {
+        const int p = s.parent[k];
+        if (p >= 0 && level[p] < level[k] + 1) {
+          level[p] = level[k] + 1;
+          changed = true;
+        }
+      }
+    }
+  }
+  int nl = 0;
+  for (int k = 0; k < nn; k++) nl = std::max(nl, level[k] + 1);
+  if (nn == 0) nl = 0;
+  std::vector<int> lptr(nl + 1, 0), lnodes(nn);
+  for (int k = 0; k < nn; k++) lptr[level[k] + 1]++;
+  for (int l = 0; l < nl; l++) lptr[l + 1] += lptr[l];
+  {
+    std::vector<int> fill(lptr.begin(), lptr.end());
+    for (int k = 0; k < nn; k++) lnodes[fill[level[k]]++] = k;
+  }
+  h->num_levels = nl;
+  h->level_ptr = lptr;
+  h->h_ns = ns;
+  h->h_nc = nc;
+  h->hp_ns = std::move(ns);
+  h->hp_nc = std::move(nc);
+  h->hp_kid_ptr = std::move(kid_ptr);
+  h->hp_kids = std::move(kids);
+  h->hp_cmap = std::move(cmap);
+  h->hp_scat_ptr = std::move(scat_ptr);
+  h->hp_scat_csr = std::move(scat_csr);
+  h->hp_scat_row = std::move(scat_row);
+  h->hp_scat_col = std::move(scat_col);
+  h->hp_level_nodes = std::move(lnodes);
+
+  // pool estimates from the symbolic fronts, scaled by the delay growth
+  double ints = 0.0, dbl = 0.0;
+  for (int k = 0; k < nn; k++) {
+    const double f = h->h_ns[k] + h->h_nc[k];
+    ints += 2.0 * f;
+    dbl += f * h->h_ns[k] + (double)h->h_nc[k] * h->h_nc[k];
+    if (f > kSmemFrontMax) dbl += f * f + 2.0 * f;
+  }
+  const double g = std::max(1.0, h->delay_growth);
+  h->icap = (unsigned long long)(ints * g * 1.5) + (1u << 16);
+  h->dcap = (unsigned long long)(dbl * g * 1.5) + (1u << 20);
+}
+
+void upload_plan(b200ldl_t h) {
+  if (h->uploaded) return;
+  const Symbolic& s = h->sym;
+  const int nn = s.num_nodes;
+  CK(h->d_ns.upload(h->hp_ns));
+  CK(h->d_nc.upload(h->hp_nc));
+  CK(h->d_var_ptr.upload(s.node_ptr));
+  CK(h->d_node_to_var.upload(s.node_to_var));
+  CK(h->d_cptr.upload(s.contrib_ptr));
+  CK(h->d_contrib_rows.upload(s.contrib_rows));
+  CK(h->d_cmap.upload(h->hp_cmap));
+  CK(h->d_kid_ptr.upload(h->hp_kid_ptr));
+  CK(h->d_kids.upload(h->hp_kids));
+  CK(h->d_scat_ptr.upload(h->hp_scat_ptr));
+  CK(h->d_scat_csr.upload(h->hp_scat_csr));
+  CK(h->d_scat_row.upload(h->hp_scat_row));
+  CK(h->d_scat_col.upload(h->hp_scat_col));
+  CK(h->d_level_nodes.upload(h->hp_level_nodes));
+
+  DevPlan& p = h->plan;
+  p.n = s.n;
+  p.num_nodes = nn;
+  p.ns = h->d_ns.ptr;
+  p.nc = h->d_nc.ptr;
+  p.var_ptr = h->d_var_ptr.ptr;
+  p.node_to_var = h->d_node_to_var.ptr;
+  p.cptr = h->d_cptr.ptr;
+  p.contrib_rows = h->d_contrib_rows.ptr;
+  p.cmap = h->d_cmap.ptr;
+  p.kid_ptr = h->d_kid_ptr.ptr;
+  p.kids = h->d_kids.ptr;
+  p.scat_ptr = h->d_scat_ptr.ptr;
+  p.scat_csr = h->d_scat_csr.ptr;
+  p.scat_row = h->d_scat_row.ptr;
+  p.scat_col = h->d_scat_col.ptr;
+
+  // per-node state
+  CK(h->d_f.alloc(nn));
+  CK(h->d_fs.alloc(nn));
+  CK(h->d_npiv.alloc(nn));
+  CK(h->d_ndel.alloc(nn));
+  CK(h->d_L_ld.alloc(nn));
+  CK(h->d_cb_ld.alloc(nn));
+  CK(h->d_fv_off.alloc(nn));
+  CK(h->d_L_off.alloc(nn));
+  CK(h->d_cb_off.alloc(nn));
+  CK(h->d_u_off.alloc(nn));
+  CK(h->d_err.alloc(4));
+  CK(h->d_inertia.alloc(2));
+  CK(h->d_flops.alloc(1));
+  CK(h->d_used.alloc(3));
+  h->uploaded = true;
+}
+
+void bind_state(b200ldl_t h) {
+  DevState& st = h->st;
+  st.f = h->d_f.ptr;
+  st.fs = h->d_fs.ptr;
+  st.npiv = h->d_npiv.ptr;
+  st.ndel = h->d_ndel.ptr;
+  st.fv_off = h->d_fv_off.ptr;
+  st.L_off = h->d_L_off.ptr;
+  st.L_ld = h->d_L_ld.ptr;
+  st.cb_off = h->d_cb_off.ptr;
+  st.cb_ld = h->d_cb_ld.ptr;
+  st.u_off = h->d_u_off.ptr;
+  st.ivars = h->d_ivars.ptr;
+  st.dpool = h->d_dpool.ptr;
+  st.used = h->d_used.ptr;
+  st.icap = h->icap;
+  st.dcap = h->dcap;
+  st.err = h->d_err.ptr;
+  st.inertia = h->d_inertia.ptr;
+  st.flops = h->d_flops.ptr;
+}
+
+void ensure_pools(b200ldl_t h) {
+  upload_plan(h);
+  if (h->d_ivars.count < h->icap) CK(h->d_ivars.alloc(h->icap));
+  if (h->d_dpool.count < h->dcap) CK(h->d_dpool.alloc(h->dcap));
+  bind_state(h);
+}
+
+void run_factor(b200ldl_t h, const double* vals, const double* diag) {
+  static bool configured = false;
+  if (!configured) {
+    CK(configure_factor_kernels());
+    CK(configure_solve_kernels());
+    configured = true;
+  }
+  FactorParams prm{h->ustab, h->pivot_tol, h->solver_type == B200LDL_CHOLESKY ? 1 : 0};
+  for (int attempt = 0; attempt < 12; attempt++) {
+    ensure_pools(h);
+    CK(cudaMemsetAsync(h->d_used.ptr, 0, 3 * sizeof(unsigned long long), h->stream));
+    CK(cudaMemsetAsync(h->d_err.ptr, 0, sizeof(int), h->stream));
+    CK(cudaMemsetAsync(h->d_err.ptr + 1, 0xff, sizeof(int), h->stream));
+    CK(cudaMemsetAsync(h->d_inertia.ptr, 0, 2 * sizeof(int), h->stream));
+    CK(cudaMemsetAsync(h->d_flops.ptr, 0, sizeof(double), h->stream));
+    CK(cudaMemsetAsync(h->d_ndel.ptr, 0, sizeof(int) * std::max(1, h->sym.num_nodes), h->stream));
+    for (int l = 0; l < h->num_levels; l++) {
+      const int b = h->level_ptr[l];
+      const int cnt = h->level_ptr[l + 1] - b;
+      launch_factor_level(h->plan, h->st, h->d_level_nodes.ptr + b, cnt, prm, h->stream,
+                          vals, diag);
+    }
+    CK(cudaGetLastError());
+    int err[2];
+    CK(cudaMemcpyAsync(err, h->d_err.ptr, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->used, h->d_used.ptr, 3 * sizeof(unsigned long long),
+                       cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(h->inertia, h->d_inertia.ptr, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaMemcpyAsync(&h->exec_flops, h->d_flops.ptr, sizeof(double), cudaMemcpyDeviceToHost,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (err[0] == 0) {
+      h->factored = true;
+      return;
+    }
+    // a pool ran out: grow both (the counters stop being meaningful after
+    // the first failure, so grow geometrically) and factor again
+    h->icap = std::max<unsigned long long>(h->icap * 2, h->used[0] + (1u << 16));
+    h->dcap = std::max<unsigned long long>(h->dcap * 2, h->used[1] + (1u << 20));
+  }
+  throw std::runtime_error("factor storage did not converge after repeated growth");
+}
+
+int max_front(b200ldl_t h) {
+  const int nn = h->sym.num_nodes;
+  std::vector<int> f(nn);
+  CK(cudaMemcpy(f.data(), h->d_f.ptr, nn * sizeof(int), cudaMemcpyDeviceToHost));
+  int m = 1;
+  for (int v : f) m = std::max(m, v);
+  return m;
+}
+
+void run_solve(b200ldl_t h, int nrhs, double* x, int ldx) {
+  if (h->fmax == 0) h->fmax = max_front(h);
+  if (h->fmax > kSolveSmemFront)
+    throw std::runtime_error("front too large for the solve kernels");
+  const size_t need = (size_t)h->used[2] * nrhs;
+  if (h->d_upool.count < need) CK(h->d_upool.alloc(need));
+  for (int l = 0; l < h->num_levels; l++) {
+    const int b = h->level_ptr[l];
+    launch_forward_level(h->plan, h->st, h->d_level_nodes.ptr + b, h->level_ptr[l + 1] - b, x,
+                         ldx, nrhs, h->d_upool.ptr, h->fmax, h->stream);
+  }
+  for (int l = h->num_levels - 1; l >= 0; l--) {
+    const int b = h->level_ptr[l];
+    launch_backward_level(h->plan, h->st, h->d_level_nodes.ptr + b, h->level_ptr[l + 1] - b, x,
+                          ldx, nrhs, h->fmax, h->stream);
+  }
+  CK(cudaGetLastError());
+}
+
+template <typename F>
+int guarded(b200ldl_t h, F&& fn) {
+  if (!h) return -1;
+  try {
+    h->last_error.clear();
+    return fn();
+  } catch (const CudaError& e) {
+    cudaGetLastError();
+    return fail(h, -3, "%s", e.what());
+  } catch (const std::bad_alloc&) {
+    return fail(h, -2, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(h, -4, "%s", e.what());
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int b200ldl_create(b200ldl_t* out, int n, int nnz, const int* rowp, const int* cols,
+                   int solver_type, double ustab, double pivot_tol, double delay_growth,
+                   int order) {
+  if (!out) return -1;
+  *out = nullptr;
+  if (n < 0 || nnz < 0 || (n > 0 && (!rowp || !cols))) return -1;
+  if (solver_type != B200LDL_LDL && solver_type != B200LDL_CHOLESKY) return -1;
+  if (order < 0 || order > 3 || order == B200LDL_ORDER_MULTI_COLOR) return -1;
+  if (n > 0 && (rowp[0] != 0 || rowp[n] != nnz)) return -1;
+  for (int i = 0; i < n; i++)
+    if (rowp[i + 1] < rowp[i]) return -1;
+  for (int e = 0; e < nnz; e++)
+    if (cols[e] < 0 || cols[e] >= n) return -1;
+  auto h = std::make_unique<b200ldl_handle>();
+  h->n = n;
+  h->nnz = nnz;
+  h->solver_type = solver_type;
+  h->ustab = ustab;
+  h->pivot_tol = pivot_tol;
+  h->delay_growth = delay_growth;
+  h->order = order;
+  int st = guarded(h.get(), [&]() {
+    h->sym = analyze(static_cast<Ordering>(order), n, rowp, cols);
+    build_plan(h.get(), rowp, cols);
+    return 0;
+  });
+  if (st != 0) {
+    std::fprintf(stderr, "b200ldl_create: %s\n", h->last_error.c_str());
+    return st;
+  }
+  *out = h.release();
+  return 0;
+}
+
+void b200ldl_destroy(b200ldl_t h) { delete h; }
+
+int b200ldl_set_stream(b200ldl_t h, void* stream) {
+  if (!h) return -1;
+  h->stream = static_cast<cudaStream_t>(stream);
+  return 0;
+}
+
+int b200ldl_factor(b200ldl_t h, const double* vals, const double* diag) {
+  return guarded(h, [&]() {
+    if (h->nnz > 0 && !vals) return fail(h, -1, "vals is null");
+    h->factored = false;
+    h->fmax = 0;
+    run_factor(h, vals, diag);
+    return 0;
+  });
+}
+
+int b200ldl_factor_host(b200ldl_t h, const double* vals, const double* diag) {
+  return guarded(h, [&]() {
+    if (h->nnz > 0 && !vals) return fail(h, -1, "vals is null");
+    if (h->d_vals.count < (size_t)std::max(1, h->nnz)) CK(h->d_vals.alloc(h->nnz));
+    CK(cudaMemcpyAsync(h->d_vals.ptr, vals, sizeof(double) * h->nnz, cudaMemcpyHostToDevice,
+                       h->stream));
+    const double* dd = nullptr;
+    if (diag) {
+      if (h->d_diag.count < (size_t)std::max(1, h->n)) CK(h->d_diag.alloc(h->n));
+      CK(cudaMemcpyAsync(h->d_diag.ptr, diag, sizeof(double) * h->n, cudaMemcpyHostToDevice,
+                         h->stream));
+      dd = h->d_diag.ptr;
+    }
+    h->factored = false;
+    h->fmax = 0;
+    run_factor(h, h->d_vals.ptr, dd);
+    return 0;
+  });
+}
+
+int b200ldl_solve(b200ldl_t h, int nrhs, double* x, int ldx) {
+  return guarded(h, [&]() {
+    if (!h->factored) return fail(h, -5, "solve called before a successful factor");
+    if (nrhs < 0 || ldx < h->n || (nrhs > 0 && !x)) return fail(h, -1, "bad solve arguments");
+    if (nrhs == 0 || h->n == 0) return 0;
+    run_solve(h, nrhs, x, ldx);
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+  });
+}
+
+int b200ldl_solve_host(b200ldl_t h, int nrhs, double* x, int ldx) {
+  return guarded(h, [&]() {
+    if (!h->factored) return fail(h, -5, "solve called before a successful factor");
+    if (nrhs < 0 || ldx < h->n || (nrhs > 0 && !x)) return fail(h, -1, "bad solve arguments");
+    if (nrhs == 0 || h->n == 0) return 0;
+    const size_t cnt = (size_t)ldx * nrhs;
+    if (h->d_x.count < cnt) CK(h->d_x.alloc(cnt));
+    CK(cudaMemcpyAsync(h->d_x.ptr, x, cnt * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    run_solve(h, nrhs, h->d_x.ptr, ldx);
+    CK(cudaMemcpyAsync(x, h->d_x.ptr, cnt * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+  });
+}
+
+int b200ldl_get_inertia(b200ldl_t h, int* npos, int* nneg) {
+  if (!h || !npos || !nneg) return -1;
+  if (!h->factored) return fail(h, -5, "inertia requested before a successful factor");
+  *npos = h->inertia[0];
+  *nneg = h->inertia[1];
+  return 0;
+}
+
+const char* b200ldl_last_error(b200ldl_t h) { return h ? h->last_error.c_str() : "null handle"; }
+
+int b200ldl_symbolic_sizes(b200ldl_t h, int* num_nodes, int* num_contrib) {
+  if (!h) return -1;
+  if (num_nodes) *num_nodes = h->sym.num_nodes;
+  if (num_contrib) *num_contrib = (int)h->sym.contrib_rows.size();
+  return 0;
+}
+
+int b200ldl_get_symbolic(b200ldl_t h, int* invperm, int* node_ptr, int* node_to_var,
+                         int* children_ptr, int* children, int* contrib_ptr,
+                         int* contrib_rows) {
+  if (!h) return -1;
+  const Symbolic& s = h->sym;
+  auto cp = [](const std::vector<int>& v, int* dst) {
+    if (dst) std::copy(v.begin(), v.end(), dst);
+  };
+  if (invperm) {
+    for (int i = 0; i < s.n; i++) invperm[i] = s.permuted ? s.iperm[i] : i;
+  }
+  cp(s.node_ptr, node_ptr);
+  cp(s.node_to_var, node_to_var);
+  cp(s.children_ptr, children_ptr);
+  if (children) std::copy(s.children.begin(), s.children.begin() + s.num_nodes, children);
+  cp(s.contrib_ptr, contrib_ptr);
+  cp(s.contrib_rows, contrib_rows);
+  return 0;
+}
+
+int b200ldl_node_pivots(b200ldl_t h, int* num_pivots, int* num_delayed) {
+  return guarded(h, [&]() {
+    if (!h->factored) return fail(h, -5, "no factorization");
+    const int nn = h->sym.num_nodes;
+    if (num_pivots) CK(cudaMemcpy(num_pivots, h->d_npiv.ptr, nn * sizeof(int), cudaMemcpyDeviceToHost));
+    if (num_delayed) CK(cudaMemcpy(num_delayed, h->d_ndel.ptr, nn * sizeof(int), cudaMemcpyDeviceToHost));
+    return 0;
+  });
+}
+
+int b200ldl_stats(b200ldl_t h, double* stats, int nstats) {
+  return guarded(h, [&]() {
+    if (!h->factored) return fail(h, -5, "no factorization");
+    const int nn = h->sym.num_nodes;
+    std::vector<int> f(nn), np(nn), nd(nn);
+    CK(cudaMemcpy(f.data(), h->d_f.ptr, nn * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(np.data(), h->d_npiv.ptr, nn * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(nd.data(), h->d_ndel.ptr, nn * sizeof(int), cudaMemcpyDeviceToHost));
+    double lbytes = 0, cbytes = 0, sdel = 0;
+    int fm = 0;
+    for (int k = 0; k < nn; k++) {
+      lbytes += 8.0 * f[k] * np[k];
+      cbytes += 8.0 * (double)(f[k] - np[k]) * (f[k] - np[k]);
+      sdel += nd[k];
+      fm = std::max(fm, f[k]);
+    }
+    const double v[6] = {h->exec_flops, lbytes, cbytes, (double)fm, sdel, (double)h->num_levels};
+    for (int i = 0; i < nstats && i < 6; i++) stats[i] = v[i];
+    return 0;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,685 @@
+// Host symbolic analysis (ordering, etree, supernodes, contribution rows).
+//
+// Each routine restates the step of the reference's symbolic phase named in
+// its comment. The integer results are the contract (they fix the front
+// structure of every supernode, hence the delayed pivots and the inertia
+// bookkeeping), so the order of operations - including tie-breaking in
+// degree lists and sorts - follows the reference step for step.
+#include "symbolic.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <numeric>
+#include <stdexcept>
+
+namespace b200ldl {
+
+namespace {
+
+// Sort, drop negative entries and duplicates; returns the new length
+// (block_amd.h:459-477).
+int sort_unique_nonneg(int len, int* a) {
+  std::sort(a, a + len);
+  int i = 0;
+  int j = 0;
+  while (i < len && a[i] < 0) i++;
+  for (; i < len; i++, j++) {
+    while (i < len - 1 && a[i] == a[i + 1]) i++;
+    if (i != j) a[j] = a[i];
+  }
+  return j;
+}
+
+// Bucketed degree lists with LIFO buckets and a monotonically non-increasing
+// minimum pointer (block_amd.h:687-812).
+struct DegreeBuckets {
+  int size;
+  int min_degree = 0;
+  std::vector<int> degree, first, next, prev;
+
+  DegreeBuckets(int size_, const int* rowp)
+      : size(size_), degree(size_), first(size_ + 1, -1), next(size_ + 1, -1),
+        prev(size_ + 1, -1) {
+    for (int i = 0; i < size; i++) {
+      degree[i] = rowp[i + 1] - rowp[i];
+      if (i == 0 || degree[i] < min_degree) min_degree = degree[i];
+    }
+    for (int i = 0; i < size; i++) push_front(i, degree[i]);
+  }
+  void push_front(int i, int d) {
+    if (first[d] != -1) {
+      prev[first[d]] = i;
+      next[i] = first[d];
+    }
+    first[d] = i;
+  }
+  void unlink(int i) {
+    const int d = degree[i];
+    if (first[d] == i) first[d] = next[i];
+    if (next[i] != -1) prev[next[i]] = prev[i];
+    if (prev[i] != -1) next[prev[i]] = next[i];
+    prev[i] = -1;
+    next[i] = -1;
+  }
+  void set(int i, int d) {
+    if (d < min_degree) min_degree = d;
+    unlink(i);
+    push_front(i, d);
+    degree[i] = d;
+  }
+  int pick() const {
+    for (int d = min_degree; d <= size; d++)
+      if (first[d] != -1) return first[d];
+    return -1;
+  }
+};
+
+// Quotient graph stored in one CSR-like array: row r holds elen[r] element
+// ids followed by (alen[r] - elen[r]) variable ids in cols[rowp[r]..].
+struct QuotientGraph {
+  int n;
+  int* rowp;
+  int* cols;
+  std::vector<int> alen, elen;
+
+  // Make room for `need` more entries at the end of row r by compacting the
+  // rows before it (towards lower addresses), then, if that is not enough,
+  // the rows after it (towards higher addresses) (block_amd.h:531-581).
+  void make_room(int r, int need) {
+    int got = 0;
+    if (r > 0) {
+      int s = r - 1;
+      for (; got < need && s >= 0; s--) got += (rowp[s + 1] - rowp[s]) - alen[s];
+      s++;
+      int dst = rowp[s] + alen[s];
+      for (int i = s + 1; i <= r; i++) {
+        int src = rowp[i];
+        const int new_start = dst;
+        const int stop = src + alen[i];
+        for (; src < stop; src++, dst++) cols[dst] = cols[src];
+        rowp[i] = new_start;
+      }
+    }
+    if (got < need) {
+      int s = r + 1;
+      for (; got < need && s < n; s++) got += (rowp[s + 1] - rowp[s]) - alen[s];
+      s--;
+      if (s >= n) {
+        s = n - 1;
+        std::fprintf(stderr, "b200ldl: quotient graph out of space\n");
+      }
+      int dst = rowp[s + 1] - 1;
+      for (int i = s; i > r; i--) {
+        const int lo = rowp[i];
+        for (int src = lo + alen[i] - 1; src >= lo; src--, dst--) cols[dst] = cols[src];
+        rowp[i] = rowp[i + 1] - alen[i];
+      }
+    }
+  }
+
+  // Indistinguishable-variable test (block_amd.h:600-630); it walks both
+  // lists in lock step, skipping the other variable once on each side.
+  bool same_adjacency(int a, int b) const {
+    if (a == b) return false;
+    if (alen[a] != alen[b] || elen[a] != elen[b]) return false;
+    int pa = rowp[a];
+    int pb = rowp[b];
+    const int ea = pa + alen[a];
+    const int eb = pb + alen[b];
+    for (int k = 0; k < alen[a]; k++, pa++, pb++) {
+      if (cols[pa] == b) pa++;
+      if (cols[pb] == a) pb++;
+      if (cols[pa] != cols[pb]) break;
+    }
+    return pa == ea && pb == eb;
+  }
+
+  // Delete variable v from the rows of its elements and neighbours
+  // (block_amd.h:637-681).
+  void drop_variable(int v) {
+    int i = rowp[v];
+    for (; i < rowp[v] + elen[v]; i++) {
+      const int e = cols[i];
+      int j = rowp[e];
+      const int last = rowp[e] + alen[e] - 1;
+      while (j < last && cols[j] != v) j++;
+      for (; j < last; j++) cols[j] = cols[j + 1];
+      alen[e]--;
+    }
+    for (; i < rowp[v] + alen[v]; i++) {
+      const int w = cols[i];
+      int j = rowp[w] + elen[w];
+      const int last = rowp[w] + alen[w] - 1;
+      while (j < last && cols[j] != v) j++;
+      for (; j < last; j++) cols[j] = cols[j + 1];
+      alen[w]--;
+    }
+    elen[v] = 0;
+    alen[v] = 0;
+  }
+};
+
+}  // namespace
+
+// Approximate minimum degree with element absorption and supervariables,
+// as BlockAMD::amd with no forced-last multipliers and the approximate
+// degree (block_amd.h:27-452, called from ordering_utils.h:202-221).
+int amd_order(int n, int* rowp, int* cols, int* perm) {
+  QuotientGraph g{n, rowp, cols, std::vector<int>(n), std::vector<int>(n, 0)};
+  std::vector<int> slen(n, 1), state(n, 1), elem_deg(n, -1), Lp(n);
+  for (int i = 0; i < n; i++) {
+    perm[i] = i;
+    g.alen[i] = rowp[i + 1] - rowp[i];
+  }
+  // input format check (strictly increasing, non-negative rows)
+  for (int i = 0; i < n; i++) {
+    for (int j = rowp[i]; j < rowp[i] + g.alen[i] - 1; j++) {
+      if (cols[j] < 0 || cols[j + 1] < 0 || cols[j + 1] <= cols[j]) return i + 1;
+    }
+  }
+
+  DegreeBuckets deg(n, rowp);
+  int nsv = 0;
+  for (int i = 0; i < n; nsv++) {
+    const int piv = deg.pick();
+    deg.unlink(piv);
+    perm[nsv] = piv;
+    state[piv] = 0;
+
+    // Lp = {piv} U adj(piv) U adj(elements of piv)
+    int len = 0;
+    Lp[len++] = piv;
+    for (int j = rowp[piv] + g.elen[piv]; j < rowp[piv] + g.alen[piv]; j++)
+      if (cols[j] != piv) Lp[len++] = cols[j];
+    for (int j = rowp[piv]; j < rowp[piv] + g.elen[piv]; j++) {
+      const int e = cols[j];
+      for (int k = rowp[e] + g.elen[e]; k < rowp[e] + g.alen[e]; k++) {
+        if (len >= n) len = sort_unique_nonneg(len, Lp.data());
+        if (cols[k] != piv) Lp[len++] = cols[k];
+      }
+    }
+    len = sort_unique_nonneg(len, Lp.data());
+
+    // prune absorbed elements and Lp members from every row in Lp
+    for (int j = 0; j < len; j++) {
+      const int v = Lp[j];
+      if (v == piv) continue;
+      int removed_e = 0;
+      {
+        int k = rowp[piv];
+        const int kend = rowp[piv] + g.elen[piv];
+        for (int c = rowp[v]; k < kend && c < rowp[v] + g.elen[v]; c++) {
+          while (k < kend && cols[k] < cols[c]) k++;
+          if (k < kend && cols[k] == cols[c]) {
+            cols[c] = -1;
+            removed_e++;
+          }
+        }
+      }
+      int removed_v = 0;
+      {
+        int k = 0;
+        for (int c = rowp[v] + g.elen[v]; k < len && c < rowp[v] + g.alen[v]; c++) {
+          while (k < len && Lp[k] < cols[c]) k++;
+          if (k < len && cols[c] == Lp[k]) {
+            cols[c] = -1;
+            removed_v++;
+          }
+        }
+      }
+      if (removed_e > 0 || removed_v > 0) {
+        const int stop = rowp[v] + g.alen[v];
+        int k = rowp[v];
+        int dst = k;
+        for (; k < stop; k++, dst++) {
+          while (k < stop && cols[k] == -1) k++;
+          if (k < stop) cols[dst] = cols[k];
+        }
+        g.elen[v] -= removed_e;
+        g.alen[v] -= removed_e + removed_v;
+      }
+    }
+
+    // piv becomes an element of every row in Lp \ {piv}, kept sorted
+    for (int j = 0; j < len; j++) {
+      const int v = Lp[j];
+      if (v == piv) continue;
+      if (g.alen[v] == rowp[v + 1] - rowp[v]) g.make_room(v, 1);
+      int k = rowp[v];
+      const int kend = k + g.elen[v];
+      while (k < kend && cols[k] < piv) k++;
+      if (cols[k] != piv) {
+        for (int p = rowp[v] + g.alen[v] - 1; p >= k; p--) cols[p + 1] = cols[p];
+        cols[k] = piv;
+        g.alen[v] += 1;
+        g.elen[v] += 1;
+      }
+    }
+
+    // the elements adjacent to piv are absorbed into it
+    for (int j = rowp[piv]; j < rowp[piv] + g.elen[piv]; j++) {
+      const int e = cols[j];
+      g.alen[e] = 0;
+      g.elen[e] = 0;
+      state[e] = -1;
+    }
+
+    // row piv now lists the variables of the new element
+    const int cap = rowp[piv + 1] - rowp[piv];
+    if (len - 1 > cap) g.make_room(piv, len - 1 - (rowp[piv + 1] - rowp[piv]));
+    g.elen[piv] = 0;
+    g.alen[piv] = len - 1;
+    for (int j = rowp[piv], k = 0; k < len; k++, j++) {
+      if (Lp[k] == piv) {
+        k++;
+        if (k == len) break;
+      }
+      cols[j] = Lp[k];
+    }
+
+    // approximate external degrees |A_v \ v| + |Lp \ v| + sum_e |L_e \ Lp|
+    for (int j = 0; j < len; j++) {
+      const int v = Lp[j];
+      for (int k = rowp[v]; k < rowp[v] + g.elen[v]; k++) {
+        const int e = cols[k];
+        if (elem_deg[e] < 0) {
+          elem_deg[e] = 0;
+          for (int p = rowp[e]; p < rowp[e] + g.alen[e]; p++) elem_deg[e] += slen[cols[p]];
+        }
+        elem_deg[e] -= slen[v];
+      }
+    }
+    int deg_lp = 0;
+    for (int j = 0; j < len; j++)
+      if (Lp[j] != piv) deg_lp += slen[Lp[j]];
+    for (int j = 0; j < len; j++) {
+      const int v = Lp[j];
+      if (v == piv) continue;
+      int est = deg_lp;
+      for (int k = rowp[v] + g.elen[v]; k < rowp[v] + g.alen[v]; k++) est += slen[cols[k]];
+      const int vs = rowp[v] + g.elen[v];
+      const int vl = g.alen[v] - g.elen[v];
+      if (vl > 0 && std::binary_search(cols + vs, cols + vs + vl, v)) est -= slen[v];
+      if (std::binary_search(Lp.data(), Lp.data() + len, v)) est -= slen[v];
+      for (int k = rowp[v]; k < rowp[v] + g.elen[v]; k++) {
+        const int e = cols[k];
+        if (e == piv) continue;
+        if (elem_deg[e] < 0) {
+          elem_deg[e] = 0;
+          for (int p = rowp[e]; p < rowp[e] + g.alen[e]; p++) elem_deg[e] += slen[cols[p]];
+        }
+        est += elem_deg[e];
+      }
+      est = std::min(est, n - i);
+      const int d = std::min(est, deg.degree[v] + deg_lp);
+      deg.set(v, d);
+    }
+    for (int j = 0; j < len; j++) {
+      const int v = Lp[j];
+      for (int k = rowp[v]; k < rowp[v] + g.elen[v]; k++) elem_deg[cols[k]] = -1;
+    }
+
+    // merge indistinguishable variables of Lp into supervariables
+    for (int j = 0; j < len; j++) {
+      const int a = Lp[j];
+      if (a == piv || slen[a] < 0) continue;
+      for (int k = j + 1; k < len; k++) {
+        const int b = Lp[k];
+        if (b == piv || slen[b] < 0) continue;
+        if (g.same_adjacency(a, b)) {
+          slen[a] += slen[b];
+          deg.set(a, deg.degree[a] - slen[b]);
+          slen[b] = -(a + 1);
+          state[b] = -1;
+          g.drop_variable(b);
+          deg.unlink(b);
+        }
+      }
+    }
+    i += slen[piv];
+  }
+
+  // expand supervariables: principal variable first, then its members in
+  // increasing index
+  int end = n;
+  for (int j = nsv - 1; j >= 0; j--) {
+    const int sv = perm[j];
+    end -= slen[sv];
+    perm[end] = sv;
+    state[sv] = end + 1;
+  }
+  for (int k = 0; k < n; k++) {
+    if (slen[k] < 0) {
+      int j = k;
+      while (slen[j] < 0) j = -(slen[j] + 1);
+      perm[state[j]] = k;
+      state[j]++;
+    }
+  }
+  return 0;
+}
+
+// copy_for_reorder (ordering_utils.h:313-360) + reorder (38-56): AMD sees the
+// pattern with the diagonal added, rows sorted and de-duplicated in place;
+// nested dissection without METIS is the identity (189-194).
+void compute_ordering(Ordering order, int n, const int* rowp, const int* cols,
+                      std::vector<int>& perm, std::vector<int>& iperm) {
+  perm.assign(n, 0);
+  iperm.assign(n, 0);
+  if (order == Ordering::Amd) {
+    const int nnz = rowp[n];
+    std::vector<int> rp(n + 1), cc(static_cast<size_t>(nnz) + n);
+    int ptr = 0;
+    rp[0] = 0;
+    for (int i = 0; i < n; i++) {
+      cc[ptr++] = i;
+      for (int jp = rowp[i]; jp < rowp[i + 1]; jp++) cc[ptr++] = cols[jp];
+      rp[i + 1] = ptr;
+    }
+    // sort_and_uniquify_csr (ordering_utils.h:812-838): rows compacted left
+    int start = rp[0];
+    for (int i = 0; i < n; i++) {
+      const int size = rp[i + 1] - start;
+      int* a = &cc[start];
+      std::sort(a, a + size);
+      int m = 0;
+      if (size > 0) {
+        cc[rp[i]] = a[0];
+        m = 1;
+        for (int r = 1; r < size; r++) {
+          if (a[r] != cc[rp[i] + m - 1]) cc[rp[i] + m++] = a[r];
+        }
+      }
+      start = rp[i + 1];
+      rp[i + 1] = rp[i] + m;
+    }
+    const int flag = amd_order(n, rp.data(), cc.data(), perm.data());
+    if (flag != 0) {
+      std::fprintf(stderr, "b200ldl: AMD input format error at row %d\n", flag - 1);
+      std::iota(perm.begin(), perm.end(), 0);
+    }
+  } else if (order == Ordering::MultiColor) {
+    throw std::invalid_argument("multicolor ordering is not supported");
+  } else {
+    std::iota(perm.begin(), perm.end(), 0);
+  }
+  for (int i = 0; i < n; i++) iperm[perm[i]] = i;
+}
+
+// compute_etree (sparse_ldl.h:2393-2458), post_order_etree +
+// depth_first_search (2473-2536), count_column_nonzeros with
+// init_column_count_data and find_root (2545-2719).
+void etree_postorder_colcount(int n, const int* rowp, const int* cols,
+                              const int* perm, const int* iperm,
+                              std::vector<int>& parent, std::vector<int>& post,
+                              std::vector<int>& colcount) {
+  parent.assign(n, -1);
+  post.assign(n, 0);
+  colcount.assign(n, 0);
+  std::vector<int> anc(n, -1);
+  for (int k = 0; k < n; k++) {
+    const int ka = perm ? perm[k] : k;
+    for (int ip = rowp[ka]; ip < rowp[ka + 1]; ip++) {
+      int i = iperm ? iperm[cols[ip]] : cols[ip];
+      while (i < k) {
+        const int up = anc[i];
+        anc[i] = k;
+        if (up == -1) {
+          parent[i] = k;
+          break;
+        }
+        i = up;
+      }
+    }
+  }
+
+  // postorder: children visited in increasing index, roots in increasing index
+  std::vector<int> head(n, -1), next(n, -1), stack(n);
+  for (int j = n - 1; j >= 0; j--) {
+    if (parent[j] != -1) {
+      next[j] = head[parent[j]];
+      head[parent[j]] = j;
+    }
+  }
+  for (int j = 0, k = 0; j < n; j++) {
+    if (parent[j] != -1) continue;
+    int top = 0;
+    stack[0] = j;
+    while (top >= 0) {
+      const int p = stack[top];
+      const int c = head[p];
+      if (c == -1) {
+        post[k++] = p;
+        top--;
+      } else {
+        head[p] = next[c];
+        stack[++top] = c;
+      }
+    }
+  }
+
+  // column counts (skeleton-graph leaves with path-compressed ancestors)
+  std::vector<int> first(n, -1), prevleaf(n, -1), maxfirst(n, -1), ancestor(n);
+  for (int k = 0; k < n; k++) {
+    int j = post[k];
+    if (first[j] == -1) colcount[j] = 1;
+    while (j != -1 && first[j] == -1) {
+      first[j] = k;
+      j = parent[j];
+    }
+  }
+  std::iota(ancestor.begin(), ancestor.end(), 0);
+  auto root_of = [&](int p) {
+    int r = p;
+    while (ancestor[r] != r) r = ancestor[r];
+    while (ancestor[p] != p) {
+      const int nx = ancestor[p];
+      ancestor[p] = r;
+      p = nx;
+    }
+    return r;
+  };
+  for (int k = 0; k < n; k++) {
+    const int j = post[k];
+    const int ja = perm ? perm[j] : j;
+    if (parent[j] != -1) colcount[parent[j]]--;
+    for (int ip = rowp[ja]; ip < rowp[ja + 1]; ip++) {
+      const int i = iperm ? iperm[cols[ip]] : cols[ip];
+      if (i <= j) continue;
+      if (first[j] <= maxfirst[i]) continue;
+      colcount[j]++;
+      maxfirst[i] = first[j];
+      const int jprev = prevleaf[i];
+      prevleaf[i] = j;
+      if (jprev != -1) colcount[root_of(jprev)]--;
+    }
+    if (parent[j] != -1) ancestor[j] = parent[j];
+  }
+  for (int k = 0; k < n; k++) {
+    const int j = post[k];
+    if (parent[j] != -1) colcount[parent[j]] += colcount[j];
+  }
+}
+
+namespace {
+
+// count_node_children (sparse_ldl.h:2978-3014): CSR of children in
+// increasing id, roots appended in slot num_nodes.
+void child_lists(int nn, const std::vector<int>& parent, std::vector<int>& ptr,
+                 std::vector<int>& kids) {
+  ptr.assign(nn + 2, 0);
+  kids.assign(std::max(nn, 1), 0);
+  for (int i = 0; i < nn; i++) {
+    const int p = parent[i];
+    ptr[(p != -1 ? p : nn) + 1]++;
+  }
+  for (int i = 0; i < nn + 1; i++) ptr[i + 1] += ptr[i];
+  for (int i = 0; i < nn; i++) {
+    const int p = parent[i];
+    const int slot = p != -1 ? p : nn;
+    kids[ptr[slot]++] = i;
+  }
+  for (int i = nn; i >= 0; i--) ptr[i + 1] = ptr[i];
+  ptr[0] = 0;
+  kids.resize(nn);
+}
+
+}  // namespace
+
+Symbolic analyze(Ordering order, int n, const int* rowp, const int* cols) {
+  Symbolic s;
+  s.n = n;
+  compute_ordering(order, n, rowp, cols, s.perm, s.iperm);
+  s.permuted = (order != Ordering::Natural);
+  const int* P = s.permuted ? s.perm.data() : nullptr;
+  const int* IP = s.permuted ? s.iperm.data() : nullptr;
+
+  std::vector<int> parent, post, colcount;
+  etree_postorder_colcount(n, rowp, cols, P, IP, parent, post, colcount);
+
+  // fundamental supernodes along the postorder (sparse_ldl.h:2734-2765)
+  std::vector<int> vtosn(n), sntov(n);
+  int nsn = 0;
+  for (int i = 0; i < n; nsn++) {
+    int var = post[i];
+    vtosn[var] = nsn;
+    sntov[i] = var;
+    i++;
+    int nv = i < n ? post[i] : n;
+    while (i < n && parent[var] == nv && colcount[nv] == colcount[var] - 1) {
+      var = nv;
+      vtosn[var] = nsn;
+      sntov[i] = var;
+      i++;
+      if (i < n) nv = post[i];
+    }
+  }
+  std::vector<int> sn_ptr(nsn + 1, 0);
+  for (int i = 0; i < n; i++) sn_ptr[vtosn[i] + 1]++;
+  for (int i = 0; i < nsn; i++) sn_ptr[i + 1] += sn_ptr[i];
+  std::vector<int> sn_parent(nsn);
+  for (int is = 0; is < nsn; is++) {
+    const int p = parent[sntov[sn_ptr[is + 1] - 1]];
+    sn_parent[is] = p >= 0 ? vtosn[p] : -1;
+  }
+  std::vector<int> sn_kptr, sn_kids;
+  child_lists(nsn, sn_parent, sn_kptr, sn_kids);
+
+  // relaxed amalgamation (sparse_ldl.h:2786-2967): children visited by
+  // increasing width of the group of the snode whose id equals the child's
+  // slot in the child array, merged while width <= 64 and the zeros added to
+  // the group stay <= 256.
+  const int max_width = 64;
+  const int max_zeros = 256;
+  std::vector<int> grp(nsn), gcount(nsn), width(nsn), zeros(nsn, 0);
+  for (int is = 0; is < nsn; is++) {
+    width[is] = sn_ptr[is + 1] - sn_ptr[is];
+    gcount[is] = colcount[sntov[sn_ptr[is]]];
+    grp[is] = is;
+  }
+  auto find = [&](int x) {
+    while (grp[x] != x) {
+      grp[x] = grp[grp[x]];
+      x = grp[x];
+    }
+    return x;
+  };
+  std::vector<int> order_buf;
+  for (int is = 0; is < nsn; is++) {
+    const int b = sn_kptr[is];
+    const int e = sn_kptr[is + 1];
+    order_buf.resize(e - b);
+    for (int ip = b; ip < e; ip++) order_buf[ip - b] = ip;
+    std::sort(order_buf.begin(), order_buf.end(),
+              [&](int x, int y) { return width[find(x)] < width[find(y)]; });
+    for (int ip : order_buf) {
+      const int child = sn_kids[ip];
+      const int rp = find(is);
+      const int rc = find(child);
+      const int w = width[rc] + width[rp];
+      if (rc != rp && w <= max_width) {
+        const int extra = std::max(0, gcount[rp] - (gcount[rc] - width[rp]));
+        const int added = extra * width[rc];
+        if (zeros[rp] + zeros[rc] + added <= max_zeros) {
+          gcount[rp] = w + gcount[rp] - width[rp];
+          width[rp] = w;
+          grp[rc] = rp;
+          zeros[rp] += added + zeros[rc];
+        }
+      }
+    }
+  }
+  std::vector<int> to_node(nsn, -1), new_id(nsn, -1);
+  int nn = 0;
+  for (int is = 0; is < nsn; is++)
+    if (find(is) == is) new_id[is] = nn++;
+  for (int is = 0; is < nsn; is++) to_node[is] = new_id[find(is)];
+
+  s.num_nodes = nn;
+  s.node_ptr.assign(nn + 1, 0);
+  s.node_to_var.assign(n, 0);
+  std::vector<int> var_to_node(n), node_count(nn);
+  for (int is = 0; is < nsn; is++) s.node_ptr[to_node[is] + 1] += sn_ptr[is + 1] - sn_ptr[is];
+  for (int k = 0; k < nn; k++) s.node_ptr[k + 1] += s.node_ptr[k];
+  {
+    std::vector<int> fill(s.node_ptr.begin(), s.node_ptr.end() - 1);
+    for (int is = 0; is < nsn; is++) {
+      const int k = to_node[is];
+      for (int ip = sn_ptr[is]; ip < sn_ptr[is + 1]; ip++) {
+        const int var = sntov[ip];
+        s.node_to_var[fill[k]++] = var;
+        var_to_node[var] = k;
+      }
+    }
+  }
+  for (int is = 0; is < nsn; is++) node_count[to_node[is]] = gcount[find(is)];
+  s.parent.assign(nn, -1);
+  for (int is = 0; is < nsn; is++) {
+    if (find(is) != is) continue;
+    const int k = to_node[is];
+    const int ps = sn_parent[is];
+    if (ps >= 0) {
+      const int kp = to_node[find(ps)];
+      if (kp != k) s.parent[k] = kp;
+    }
+  }
+  child_lists(nn, s.parent, s.children_ptr, s.children);
+
+  // contribution rows (sparse_ldl.h:2323-2348, build_nonzero_pattern
+  // 3036-3122): walk each row's subtree upward, one visit per node per row
+  s.contrib_ptr.assign(nn + 1, 0);
+  for (int k = 0; k < nn; k++) s.contrib_ptr[k + 1] = node_count[k] - (s.node_ptr[k + 1] - s.node_ptr[k]);
+  for (int k = 0; k < nn; k++) s.contrib_ptr[k + 1] += s.contrib_ptr[k];
+  s.contrib_rows.assign(s.contrib_ptr[nn], 0);
+  {
+    std::vector<int> filled(nn, 0), flag(nn, -1), up(nn);
+    for (int k = 0; k < nn; k++) {
+      const int last = s.node_to_var[s.node_ptr[k + 1] - 1];
+      const int p = parent[last];
+      up[k] = p >= 0 ? var_to_node[p] : -1;
+    }
+    for (int k = 0; k < n; k++) {
+      const int ks = var_to_node[k];
+      const int ka = P ? P[k] : k;
+      for (int ip = rowp[ka]; ip < rowp[ka + 1]; ip++) {
+        const int i = IP ? IP[cols[ip]] : cols[ip];
+        if (i >= k) continue;
+        for (int is = var_to_node[i]; is >= 0 && is != ks; is = up[is]) {
+          if (flag[is] == k) break;
+          flag[is] = k;
+          const int pos = s.contrib_ptr[is] + filled[is];
+          if (pos >= s.contrib_ptr[is + 1])
+            throw std::runtime_error("symbolic: contribution row overflow");
+          s.contrib_rows[pos] = ka;
+          filled[is]++;
+        }
+      }
+    }
+  }
+  if (P) {
+    for (int i = 0; i < n; i++) s.node_to_var[i] = P[s.node_to_var[i]];
+  }
+  return s;
+}
+
+}  // namespace b200ldl

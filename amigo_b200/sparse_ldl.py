@@ -1,0 +1,282 @@
+"""Host-side mirror of the reference's SparseLDL interface, running on the GPU.
+
+``SparseLDL(mat, solver_type, ustab, pivot_tol, delay_growth, order)`` with
+``factor(diagonal=None)``, ``solve(x)`` and ``get_inertia()`` behaves like the
+pybind class of the same name (amigo/amigo.cpp:648-732 over
+include/sparse_ldl.h:65-213): the symbolic phase runs on the host when the
+object is built, ``factor`` returns 0, ``solve`` overwrites its argument,
+``get_inertia`` returns ``(npos, nneg)``. The numeric work runs in the
+sm_100a kernels of libb200ldl.so; there is no CPU path.
+
+Accepted value containers: numpy arrays (host; copied to the device inside
+the call) and torch CUDA tensors (used in place on the device).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import enum
+
+import numpy as np
+
+from . import _native
+
+__all__ = ["SolverType", "OrderingType", "CSRMat", "Vector", "SparseLDL"]
+
+
+class SolverType(enum.IntEnum):
+    LDL = 0
+    CHOLESKY = 1
+
+
+class OrderingType(enum.IntEnum):
+    NESTED_DISSECTION = 0
+    AMD = 1
+    MULTI_COLOR = 2
+    NATURAL = 3
+    # the reference's DEFAULT without METIS (amigo/amigo.cpp:329-333)
+    DEFAULT = 1
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+class CSRMat:
+    """Symmetric CSR matrix (full pattern), as amigo.CSRMat's constructor
+    ``CSRMat(nrows, ncols, rowp, cols, vals)`` (amigo/amigo.cpp:346-381).
+    ``vals`` may be a numpy array or a torch CUDA tensor."""
+
+    def __init__(self, nrows, ncols, rowp, cols, vals=None):
+        self.nrows = int(nrows)
+        self.ncols = int(ncols)
+        self.rowp = np.ascontiguousarray(rowp, dtype=np.int32)
+        self.cols = np.ascontiguousarray(cols, dtype=np.int32)
+        if self.rowp.shape != (self.nrows + 1,):
+            raise RuntimeError("rowp must have length nrows + 1")
+        nnz = int(self.rowp[-1])
+        if vals is None:
+            vals = np.zeros(nnz)
+        if not _is_torch(vals):
+            vals = np.ascontiguousarray(vals, dtype=np.float64)
+        if len(self.cols) != nnz or vals.shape[0] != nnz:
+            raise RuntimeError("cols and vals must have the same length")
+        self.vals = vals
+
+    @property
+    def nnz(self) -> int:
+        return int(self.rowp[-1])
+
+    def get_nonzero_structure(self):
+        return self.nrows, self.ncols, self.nnz, self.rowp.copy(), self.cols.copy()
+
+    def get_data(self):
+        return self.vals
+
+
+class Vector:
+    """Minimal stand-in for amigo.Vector: a length-n float64 array (numpy or a
+    torch CUDA tensor) with item access."""
+
+    def __init__(self, n_or_array):
+        if isinstance(n_or_array, (int, np.integer)):
+            self.array = np.zeros(int(n_or_array))
+        else:
+            self.array = n_or_array
+
+    def get_size(self) -> int:
+        return int(self.array.shape[0])
+
+    def get_array(self):
+        return self.array
+
+    def __getitem__(self, i):
+        return self.array[i]
+
+    def __setitem__(self, i, v):
+        self.array[i] = v
+
+
+def _values_of(obj):
+    """numpy/torch array behind a CSRMat, Vector, amigo object or array."""
+    if obj is None:
+        return None
+    if isinstance(obj, CSRMat):
+        return obj.vals
+    if isinstance(obj, Vector):
+        return obj.array
+    if hasattr(obj, "get_data") and not isinstance(obj, np.ndarray) and not _is_torch(obj):
+        return np.asarray(obj.get_data())  # amigo.CSRMat (host view)
+    if hasattr(obj, "get_size") and hasattr(obj, "__getitem__") and not _is_torch(obj) \
+            and not isinstance(obj, np.ndarray):
+        return np.asarray(obj[:], dtype=np.float64)  # amigo.Vector
+    return obj
+
+
+class SparseLDL:
+    """GPU multifrontal LDL^T with the reference SparseLDL's interface."""
+
+    def __init__(self, mat, solver_type=SolverType.LDL, ustab: float = 0.01,
+                 pivot_tol: float = 1e-14, delay_growth: float = 2.0,
+                 order=OrderingType.NATURAL):
+        self._lib = _native.load()
+        if isinstance(mat, CSRMat):
+            rowp, cols = mat.rowp, mat.cols
+            n = mat.nrows
+        else:  # an amigo.CSRMat
+            n, _, _, rowp, cols = mat.get_nonzero_structure()
+        self.mat = mat
+        self.n = int(n)
+        self.rowp = np.ascontiguousarray(rowp, dtype=np.int32)
+        self.cols = np.ascontiguousarray(cols, dtype=np.int32)
+        self.nnz = int(self.rowp[-1])
+        self.solver_type = SolverType(int(solver_type))
+        self.order = int(order)
+        h = ctypes.c_void_p()
+        st = self._lib.b200ldl_create(
+            ctypes.byref(h), self.n, self.nnz,
+            self.rowp.ctypes.data_as(_native._i32p), self.cols.ctypes.data_as(_native._i32p),
+            int(self.solver_type), float(ustab), float(pivot_tol), float(delay_growth),
+            self.order)
+        if st != 0:
+            raise _native.NativeError(f"b200ldl_create failed with status {st}", st)
+        self._h = h
+        self._keep = []
+
+    # -- lifetime -----------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.b200ldl_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- numeric phase -------------------------------------------------------
+    def factor(self, diagonal=None) -> int:
+        vals = _values_of(self.mat)
+        diag = _values_of(diagonal)
+        if _is_torch(vals):
+            import torch
+
+            if not vals.is_cuda:
+                vals = vals.numpy()
+            else:
+                vals = vals.contiguous().to(torch.float64)
+                if diag is not None:
+                    if not _is_torch(diag):
+                        diag = torch.as_tensor(np.asarray(diag, np.float64), device=vals.device)
+                    diag = diag.contiguous().to(device=vals.device, dtype=torch.float64)
+                self._keep = [vals, diag]
+                self._sync_stream(vals)
+                st = self._lib.b200ldl_factor(
+                    self._h, ctypes.c_void_p(vals.data_ptr()),
+                    ctypes.c_void_p(diag.data_ptr()) if diag is not None else None)
+                return _native.check(self._h, st, "factor")
+        v = np.ascontiguousarray(vals, dtype=np.float64)
+        d = None if diag is None else np.ascontiguousarray(
+            diag.cpu().numpy() if _is_torch(diag) else diag, dtype=np.float64)
+        st = self._lib.b200ldl_factor_host(
+            self._h, v.ctypes.data_as(_native._f64p),
+            d.ctypes.data_as(_native._f64p) if d is not None else None)
+        return _native.check(self._h, st, "factor")
+
+    def _sync_stream(self, t):
+        import torch
+
+        stream = torch.cuda.current_stream(t.device)
+        self._lib.b200ldl_set_stream(self._h, ctypes.c_void_p(stream.cuda_stream))
+
+    def solve(self, x):
+        """Overwrite x (Vector, numpy 1D/2D, or torch CUDA tensor 1D/2D with
+        the n rows first) with K^{-1} x."""
+        arr = _values_of(x)
+        if _is_torch(arr) and arr.is_cuda:
+            import torch
+
+            if arr.dtype != torch.float64:
+                raise TypeError("solve needs float64")
+            nrhs = 1 if arr.dim() == 1 else arr.shape[1]
+            if arr.dim() == 1:
+                work = arr if arr.is_contiguous() else arr.contiguous()
+                ldx = self.n
+            else:
+                # column-major n x nrhs == row-major nrhs x n
+                if arr.stride(0) == 1 and arr.stride(1) >= self.n:
+                    work = arr
+                    ldx = arr.stride(1)
+                else:
+                    work = arr.t().contiguous().t()
+                    ldx = self.n
+            self._sync_stream(work)
+            st = self._lib.b200ldl_solve(self._h, nrhs, ctypes.c_void_p(work.data_ptr()), ldx)
+            _native.check(self._h, st, "solve")
+            if work.data_ptr() != arr.data_ptr():
+                arr.copy_(work)
+            return None
+        a = np.asarray(arr)
+        if a.dtype != np.float64:
+            raise TypeError("NumPy array must have dtype=float64")
+        nrhs = 1 if a.ndim == 1 else a.shape[1]
+        f = np.asfortranarray(a)
+        st = self._lib.b200ldl_solve_host(self._h, nrhs, f.ctypes.data_as(_native._f64p),
+                                          self.n)
+        _native.check(self._h, st, "solve")
+        if not np.shares_memory(f, a):
+            a[...] = f
+        if isinstance(x, Vector) and x.array is not a:
+            x.array[...] = a
+        elif not isinstance(x, (np.ndarray, Vector)) and hasattr(x, "__setitem__"):
+            x[:] = a
+        return None
+
+    def get_inertia(self):
+        p = ctypes.c_int()
+        q = ctypes.c_int()
+        st = self._lib.b200ldl_get_inertia(self._h, ctypes.byref(p), ctypes.byref(q))
+        _native.check(self._h, st, "get_inertia")
+        if self.solver_type == SolverType.CHOLESKY:
+            return (0, 0)
+        return (p.value, q.value)
+
+    # -- introspection used by the parity tests --------------------------------
+    def symbolic(self) -> dict:
+        nn = ctypes.c_int()
+        nc = ctypes.c_int()
+        self._lib.b200ldl_symbolic_sizes(self._h, ctypes.byref(nn), ctypes.byref(nc))
+        nn, nc = nn.value, nc.value
+        out = {
+            "invperm": np.empty(self.n, np.int32),
+            "node_ptr": np.empty(nn + 1, np.int32),
+            "node_to_var": np.empty(self.n, np.int32),
+            "children_ptr": np.empty(nn + 2, np.int32),
+            "children": np.empty(max(nn, 1), np.int32),
+            "contrib_ptr": np.empty(nn + 1, np.int32),
+            "contrib_rows": np.empty(max(nc, 1), np.int32),
+        }
+        keys = ("invperm", "node_ptr", "node_to_var", "children_ptr", "children",
+                "contrib_ptr", "contrib_rows")
+        self._lib.b200ldl_get_symbolic(self._h, *[out[k].ctypes.data_as(_native._i32p)
+                                                  for k in keys])
+        out["children"] = out["children"][:nn]
+        out["contrib_rows"] = out["contrib_rows"][:nc]
+        return out
+
+    def node_pivots(self):
+        nn = len(self.symbolic()["node_ptr"]) - 1
+        a = np.empty(nn, np.int32)
+        b = np.empty(nn, np.int32)
+        st = self._lib.b200ldl_node_pivots(self._h, a.ctypes.data_as(_native._i32p),
+                                           b.ctypes.data_as(_native._i32p))
+        _native.check(self._h, st, "node_pivots")
+        return a, b
+
+    def stats(self) -> dict:
+        v = np.zeros(6)
+        st = self._lib.b200ldl_stats(self._h, v.ctypes.data_as(_native._f64p), 6)
+        _native.check(self._h, st, "stats")
+        return {"flops": v[0], "L_bytes": v[1], "cb_bytes": v[2], "max_front": int(v[3]),
+                "delayed": int(v[4]), "levels": int(v[5])}

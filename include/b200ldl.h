@@ -1,0 +1,116 @@
+/*
+ * b200ldl: B200 (sm_100a) supernodal multifrontal LDL^T / Cholesky for
+ * Amigo's interior-point KKT systems  K = [[H + Sigma, A^T], [A, -delta I]].
+ *
+ * C ABI. Plain pointers and sizes only. Every call returns an int status:
+ *   0   success
+ *   >0  numerical condition (see b200ldl_last_error)
+ *   <0  argument, allocation or CUDA error (the handle stays usable)
+ * Nothing aborts the process.
+ *
+ * Matrix convention (same as the reference's CSRMat input to SparseLDL):
+ * one CSR over all n variables holding the FULL symmetric pattern, 0-based
+ * int32 indices, double values, every row containing its diagonal. The
+ * optional diagonal vector `diag` is added to the diagonal during the
+ * factorization (Amigo passes Sigma + delta_w on primal rows and -delta_c on
+ * constraint rows this way).
+ *
+ * Each entry point names the reference interface it replaces
+ * (Mersoltane/amigo, paths relative to the repository root).
+ */
+#ifndef B200LDL_H
+#define B200LDL_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct b200ldl_handle* b200ldl_t;
+
+/* Solver type, as amigo::SparseLDL<T>::SolverType (include/sparse_ldl.h:23). */
+#define B200LDL_LDL 0
+#define B200LDL_CHOLESKY 1
+
+/* Orderings, numbered as amigo::OrderingType (include/ordering_utils.h:21).
+ * NESTED_DISSECTION is the identity (the reference without METIS,
+ * include/ordering_utils.h:189-194); MULTI_COLOR is rejected. */
+#define B200LDL_ORDER_NESTED_DISSECTION 0
+#define B200LDL_ORDER_AMD 1
+#define B200LDL_ORDER_MULTI_COLOR 2
+#define B200LDL_ORDER_NATURAL 3
+
+/* Create a solver for a fixed sparsity pattern and run the symbolic phase on
+ * the host (ordering, elimination tree, supernodes, contribution rows), then
+ * upload the assembly and extend-add maps to the current CUDA device.
+ * rowp/cols are host arrays. Replaces SparseLDL::SparseLDL
+ * (include/sparse_ldl.h:65-118); defaults there are ustab = 0.01,
+ * pivot_tol = 1e-14, delay_growth = 2.0. */
+int b200ldl_create(b200ldl_t* out, int n, int nnz, const int* rowp,
+                   const int* cols, int solver_type, double ustab,
+                   double pivot_tol, double delay_growth, int order);
+
+/* Release the handle and its device memory. */
+void b200ldl_destroy(b200ldl_t h);
+
+/* Run subsequent work on this cudaStream_t (0 = the legacy default stream). */
+int b200ldl_set_stream(b200ldl_t h, void* stream);
+
+/* Numeric factorization of the CSR values `vals` [nnz] plus the optional
+ * diagonal `diag` [n] (NULL for none); both are DEVICE pointers. Threshold
+ * 1x1/2x2 pivoting with delayed pivots inside fronts, Bunch-Kaufman at
+ * roots. Replaces SparseLDL::factor (include/sparse_ldl.h:136-158) and, for
+ * device-resident data, CSRMatFactorCuda::factor
+ * (include/cuda/csr_factor_cuda.h:13-35). Synchronizes the handle's stream. */
+int b200ldl_factor(b200ldl_t h, const double* vals, const double* diag);
+
+/* Same with HOST vals/diag (copied in on the handle's stream). */
+int b200ldl_factor_host(b200ldl_t h, const double* vals, const double* diag);
+
+/* Solve K x = b in place for nrhs right-hand sides stored column-major with
+ * leading dimension ldx >= n (DEVICE pointer). Replaces
+ * SparseLDL::solve(int nrhs, T* x, int ldx) (include/sparse_ldl.h:191-197)
+ * and CSRMatFactorCuda::solve. K is symmetric, so this is also the
+ * transposed (adjoint) solve. */
+int b200ldl_solve(b200ldl_t h, int nrhs, double* x, int ldx);
+
+/* Same with a HOST array x (copied in and out). */
+int b200ldl_solve_host(b200ldl_t h, int nrhs, double* x, int ldx);
+
+/* Inertia of the last factorization: numbers of positive and negative
+ * pivots (zero pivots count as positive, as the reference does). Replaces
+ * SparseLDL::get_inertia (include/sparse_ldl.h:205-213). */
+int b200ldl_get_inertia(b200ldl_t h, int* npos, int* nneg);
+
+/* Message for the last non-zero status on this handle ("" if none). */
+const char* b200ldl_last_error(b200ldl_t h);
+
+/* Sizes of the symbolic structure: number of supernodes and total number
+ * of contribution rows. */
+int b200ldl_symbolic_sizes(b200ldl_t h, int* num_nodes, int* num_contrib);
+
+/* Copy the symbolic structure to host arrays (any pointer may be NULL):
+ * invperm [n], node_ptr [num_nodes+1], node_to_var [n], children_ptr
+ * [num_nodes+2] (roots in slot num_nodes), children [num_nodes],
+ * contrib_ptr [num_nodes+1], contrib_rows [num_contrib]. Same layout and
+ * numbering as the reference's SparseLDL members (include/sparse_ldl.h:
+ * 3269-3286). */
+int b200ldl_get_symbolic(b200ldl_t h, int* invperm, int* node_ptr,
+                         int* node_to_var, int* children_ptr, int* children,
+                         int* contrib_ptr, int* contrib_rows);
+
+/* Per-supernode pivot and delayed-pivot counts of the last factorization
+ * (host arrays of length num_nodes). */
+int b200ldl_node_pivots(b200ldl_t h, int* num_pivots, int* num_delayed);
+
+/* Statistics of the last factorization: stats[0] = factor flops actually
+ * executed (dense partial factorizations of the fronts as sized at run
+ * time), stats[1] = bytes of the factor L, stats[2] = bytes of the
+ * contribution blocks, stats[3] = largest front, stats[4] = number of
+ * delayed pivots summed over supernodes, stats[5] = number of levels. */
+int b200ldl_stats(b200ldl_t h, double* stats, int nstats);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200LDL_H */
