@@ -83,6 +83,7 @@ struct b200ldl_handle {
   std::vector<int64_t> hp_scat_ptr;
   int num_levels = 0;
   std::vector<int> level_ptr;  // host copy
+  std::vector<int> level_maxkids;
   std::vector<int> h_ns, h_nc;
 
   // device plan
@@ -96,6 +97,9 @@ struct b200ldl_handle {
   DevBuf<int64_t> d_fv_off, d_L_off, d_cb_off, d_u_off;
   DevBuf<double> d_dpool, d_flops, d_upool, d_vals, d_diag, d_x;
   DevBuf<unsigned long long> d_used;
+  DevBuf<BigFront> d_big;
+  DevBuf<int> d_big_meta;
+  DevBuf<long long> d_tile_ptr;
   unsigned long long icap = 0, dcap = 0;
   DevState st{};
 
@@ -215,6 +219,12 @@ void build_plan(b200ldl_t h, const int* rowp, const int* cols) {
   }
   h->num_levels = nl;
   h->level_ptr = lptr;
+  h->level_maxkids.assign(nl, 0);
+  for (int l = 0; l < nl; l++)
+    for (int q = lptr[l]; q < lptr[l + 1]; q++) {
+      const int k = lnodes[q];
+      h->level_maxkids[l] = std::max(h->level_maxkids[l], kid_ptr[k + 1] - kid_ptr[k]);
+    }
   h->h_ns = ns;
   h->h_nc = nc;
   h->hp_ns = std::move(ns);
@@ -292,6 +302,9 @@ void upload_plan(b200ldl_t h) {
   CK(h->d_inertia.alloc(2));
   CK(h->d_flops.alloc(1));
   CK(h->d_used.alloc(3));
+  CK(h->d_big.alloc(nn));
+  CK(h->d_big_meta.alloc(4));
+  CK(h->d_tile_ptr.alloc(nn + 1));
   h->uploaded = true;
 }
 
@@ -315,6 +328,9 @@ void bind_state(b200ldl_t h) {
   st.err = h->d_err.ptr;
   st.inertia = h->d_inertia.ptr;
   st.flops = h->d_flops.ptr;
+  st.big = h->d_big.ptr;
+  st.big_meta = h->d_big_meta.ptr;
+  st.tile_ptr = h->d_tile_ptr.ptr;
 }
 
 void ensure_pools(b200ldl_t h) {
@@ -329,6 +345,7 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
   if (!configured) {
     CK(configure_factor_kernels());
     CK(configure_solve_kernels());
+    CK(configure_big_kernels());
     configured = true;
   }
   FactorParams prm{h->ustab, h->pivot_tol, h->solver_type == B200LDL_CHOLESKY ? 1 : 0};
@@ -343,8 +360,19 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
     for (int l = 0; l < h->num_levels; l++) {
       const int b = h->level_ptr[l];
       const int cnt = h->level_ptr[l + 1] - b;
+      CK(cudaMemsetAsync(h->d_big_meta.ptr, 0, 4 * sizeof(int), h->stream));
       launch_factor_level(h->plan, h->st, h->d_level_nodes.ptr + b, cnt, prm, h->stream,
                           vals, diag);
+      CK(cudaGetLastError());
+      int meta[4];
+      CK(cudaMemcpyAsync(meta, h->d_big_meta.ptr, 4 * sizeof(int), cudaMemcpyDeviceToHost,
+                         h->stream));
+      CK(cudaStreamSynchronize(h->stream));
+      if (meta[0] > 0) {
+        BigLevelInfo info{meta[0], meta[1], meta[2]};
+        CK(launch_big_level(h->plan, h->st, info, h->level_maxkids[l], prm, vals, diag,
+                            h->stream));
+      }
     }
     CK(cudaGetLastError());
     int err[2];

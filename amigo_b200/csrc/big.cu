@@ -1,0 +1,759 @@
+// Fronts too large for one CTA's shared memory.
+//
+// Each big front F (f x f, column-major, lower triangle used) lives in the
+// device pool. Its fully summed candidates are factored panel by panel with
+// the reference's blocked algorithm (SparseLDL::factor_front_matrix_block,
+// include/sparse_ldl.h:1316-1553): within a panel the next candidate column
+// is formed on the fly as F(:,k) - Lp W(k,:)^T, tested (1x1, alternative
+// 1x1 at imax, Duff 2x2, or delay; Bunch-Kaufman when the front has no
+// contribution rows), and accepted columns are appended to the panel; after
+// the panel the trailing matrix receives one rank-kw update.
+//
+// B200 mapping: the panel of one front is owned by a thread-block cluster
+// (4, 8 or 16 CTAs). Rows are split in contiguous blocks across the CTAs and
+// each CTA keeps its rows of the panel's L and W columns in shared memory,
+// so the per-column GEMV never leaves the SM. Column maxima are reduced
+// across the cluster through distributed shared memory, and every CTA makes
+// the same pivot decision from the same reduced values, so all CTAs run the
+// same sequence of cluster barriers. The trailing update is a separate
+// tiled FP64 kernel over all big fronts of the level.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <climits>
+
+#include "ldl_internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace b200ldl {
+
+namespace {
+
+constexpr int kPanelThreads = 256;
+constexpr int kPWarps = kPanelThreads / 32;
+constexpr int kTile = 64;
+constexpr int kUpdThreads = 256;
+
+__device__ __forceinline__ void keep_larger(double& bv, int& bi, double v, int i) {
+  if (v > bv || (v == bv && i < bi)) {
+    bv = v;
+    bi = i;
+  }
+}
+
+struct Part {
+  double v;  // best |.| among candidates
+  int i;     // its row
+  int pad;
+  double m;  // max |.| among contribution rows / row max
+  double x;  // a value owned by this CTA (diagonal etc.)
+  double y;
+};
+
+struct BlockRed {
+  double v[kPWarps];
+  int i[kPWarps];
+  double m[kPWarps];
+};
+
+__device__ void block_reduce(BlockRed& r, double& bv, int& bi, double& cm) {
+  const int lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_down_sync(0xffffffffu, bv, o);
+    const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+    const double om = __shfl_down_sync(0xffffffffu, cm, o);
+    keep_larger(bv, bi, ov, oi);
+    cm = fmax(cm, om);
+  }
+  if (lane == 0) {
+    r.v[w] = bv;
+    r.i[w] = bi;
+    r.m[w] = cm;
+  }
+  __syncthreads();
+  bv = r.v[0];
+  bi = r.i[0];
+  cm = r.m[0];
+#pragma unroll
+  for (int q = 1; q < kPWarps; q++) {
+    keep_larger(bv, bi, r.v[q], r.i[q]);
+    cm = fmax(cm, r.m[q]);
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------- assembly
+
+__global__ void big_zero_kernel(DevState s) {
+  const BigFront& B = s.big[blockIdx.x];
+  double* F = s.dpool + B.doff;
+  const int f = B.f;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  for (int j = blockIdx.y * nw + warp; j < f; j += gridDim.y * nw) {
+    double* col = F + (size_t)f * j;
+    for (int i = j + lane; i < f; i += 32) col[i] = 0.0;
+  }
+}
+
+__global__ void big_scatter_kernel(DevPlan p, DevState s, const double* __restrict__ vals,
+                                   const double* __restrict__ diag) {
+  const BigFront& B = s.big[blockIdx.x];
+  double* F = s.dpool + B.doff;
+  const int f = B.f, ns = B.ns, nd_in = B.nd_in, node = B.node;
+  const int64_t e0 = p.scat_ptr[node];
+  const int64_t e1 = p.scat_ptr[node + 1];
+  const int64_t stride = (int64_t)gridDim.y * blockDim.x;
+  for (int64_t e = e0 + (int64_t)blockIdx.y * blockDim.x + threadIdx.x; e < e1; e += stride) {
+    int r = p.scat_row[e];
+    if (r >= ns) r += nd_in;
+    F[r + (size_t)f * p.scat_col[e]] += vals[p.scat_csr[e]];
+  }
+}
+
+__global__ void big_diag_kernel(DevPlan p, DevState s, const double* __restrict__ diag) {
+  const BigFront& B = s.big[blockIdx.x];
+  double* F = s.dpool + B.doff;
+  const int f = B.f;
+  const int v0 = p.var_ptr[B.node];
+  for (int j = threadIdx.x; j < B.ns; j += blockDim.x)
+    F[j + (size_t)f * j] += diag[p.node_to_var[v0 + j]];
+}
+
+// extend-add of the c-th child of every big front
+__global__ void big_extend_kernel(DevPlan p, DevState s, int c) {
+  const BigFront& B = s.big[blockIdx.x];
+  const int node = B.node;
+  const int kb = p.kid_ptr[node];
+  const int ke = p.kid_ptr[node + 1];
+  if (kb + c >= ke) return;
+  double* F = s.dpool + B.doff;
+  const int f = B.f, ns = B.ns, nd_in = B.nd_in;
+  int off = ns;
+  for (int q = kb; q < kb + c; q++) off += s.ndel[p.kids[q]];
+  const int ch = p.kids[kb + c];
+  const int nd = s.ndel[ch];
+  const int m = s.f[ch] - s.npiv[ch];
+  const double* cb = s.dpool + s.cb_off[ch];
+  const int cld = s.cb_ld[ch];
+  const int* cm = p.cmap + p.cptr[ch];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  for (int r2 = blockIdx.y * nw + warp; r2 < m; r2 += gridDim.y * nw) {
+    int p2;
+    if (r2 < nd) {
+      p2 = off + r2;
+    } else {
+      p2 = cm[r2 - nd];
+      if (p2 >= ns) p2 += nd_in;
+    }
+    const double* col = cb + (size_t)cld * r2;
+    for (int r1 = r2 + lane; r1 < m; r1 += 32) {
+      int p1;
+      if (r1 < nd) {
+        p1 = off + r1;
+      } else {
+        p1 = cm[r1 - nd];
+        if (p1 >= ns) p1 += nd_in;
+      }
+      const double v = col[r1];
+      if (p1 >= p2)
+        F[p1 + (size_t)f * p2] += v;
+      else
+        F[p2 + (size_t)f * p1] += v;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ panel
+
+// Symmetric interchange of rows/columns a < b: the front in global memory
+// (all CTAs of the cluster share the element range), the panel rows held in
+// shared memory (exchanged by the owner of row a through DSMEM), and the
+// front-variable / original-position lists.
+template <int CL>
+__device__ void cluster_swap(cg::cluster_group& cl, int rank, double* F, int f, int* fv,
+                             int* orig, int a, int b, int R, int NB, int kw, double* Lp,
+                             double* Wp, double* wc0, double* wc1) {
+  const int n1 = a;
+  const int n2 = b - a - 1;
+  const int n3 = f - b - 1;
+  const int total = n1 + 1 + n2 + n3;
+  for (int t = rank * blockDim.x + threadIdx.x; t < total; t += CL * blockDim.x) {
+    double *p, *q;
+    if (t < n1) {
+      p = &F[a + (size_t)f * t];
+      q = &F[b + (size_t)f * t];
+    } else if (t == n1) {
+      p = &F[a + (size_t)f * a];
+      q = &F[b + (size_t)f * b];
+    } else if (t < n1 + 1 + n2) {
+      const int j = a + 1 + (t - n1 - 1);
+      p = &F[j + (size_t)f * a];
+      q = &F[b + (size_t)f * j];
+    } else {
+      const int j = b + 1 + (t - n1 - 1 - n2);
+      p = &F[j + (size_t)f * a];
+      q = &F[j + (size_t)f * b];
+    }
+    const double tmp = *p;
+    *p = *q;
+    *q = tmp;
+  }
+  const int oa = a / R;
+  const int ob = b / R;
+  if (rank == oa) {
+    double* La = Lp + (size_t)(a - oa * R) * NB;
+    double* Wa = Wp + (size_t)(a - oa * R) * NB;
+    double* Lb = cl.map_shared_rank(Lp, ob) + (size_t)(b - ob * R) * NB;
+    double* Wb = cl.map_shared_rank(Wp, ob) + (size_t)(b - ob * R) * NB;
+    for (int j = threadIdx.x; j < kw; j += blockDim.x) {
+      double t = La[j];
+      La[j] = Lb[j];
+      Lb[j] = t;
+      t = Wa[j];
+      Wa[j] = Wb[j];
+      Wb[j] = t;
+    }
+    if (threadIdx.x == 0) {
+      double* x0 = cl.map_shared_rank(wc0, ob) + (b - ob * R);
+      double* x1 = cl.map_shared_rank(wc1, ob) + (b - ob * R);
+      double t = wc0[a - oa * R];
+      wc0[a - oa * R] = *x0;
+      *x0 = t;
+      t = wc1[a - oa * R];
+      wc1[a - oa * R] = *x1;
+      *x1 = t;
+    }
+  }
+  if (rank == 0 && threadIdx.x == 0) {
+    int t = fv[a];
+    fv[a] = fv[b];
+    fv[b] = t;
+    t = orig[a];
+    orig[a] = orig[b];
+    orig[b] = t;
+  }
+}
+
+enum : int { kDelay = 0, kOne = 1, kTwo = 2, kNeedRow = 3, kZero = 4 };
+
+template <int CL>
+__global__ void __launch_bounds__(kPanelThreads)
+    big_panel_kernel(DevState s, FactorParams prm, int NB) {
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  BigFront* B = s.big + blockIdx.x / CL;
+  extern __shared__ __align__(16) double sm[];
+  __shared__ Part partA, partB;
+  __shared__ BlockRed red;
+  __shared__ double wk[kBigPanelMax], wi[kBigPanelMax];
+  __shared__ int dec[4];
+  __shared__ double dval[8];
+
+  const int tid = threadIdx.x;
+  if (B->state != 0) return;  // same value in every CTA of the cluster
+  const int f = B->f;
+  const bool root = (B->nc == 0);
+  int k = B->k;
+  int ncand = B->ncand;
+  const int R = (f + CL - 1) / CL;
+  const int r0 = rank * R;
+  const int r1 = min(f, r0 + R);
+  double* Lp = sm;
+  double* Wp = Lp + (size_t)R * NB;
+  double* wc0 = Wp + (size_t)R * NB;
+  double* wc1 = wc0 + R;
+  double* F = s.dpool + B->doff;
+  double* Wg = s.dpool + B->woff;
+  int* fv = s.ivars + B->ioff;
+  int* orig = fv + f;
+  const double alpha_bk = (1.0 + 4.1231056256176605) / 8.0;  // (1 + sqrt(17)) / 8
+  const int kstart = k;
+  int kw = 0;
+  int npos = 0, nneg = 0;
+  double flops = 0.0;
+
+  while (kw < NB - 1 && k < ncand) {
+    const int ok = k / R;
+    if (tid < kw) wk[tid] = cl.map_shared_rank(Wp, ok)[(size_t)(k - ok * R) * NB + tid];
+    __syncthreads();
+    // candidate column k on this CTA's rows
+    double bv = -1.0, cm = 0.0;
+    int bi = INT_MAX;
+    const int lo = max(r0, k);
+    for (int i = lo + tid; i < r1; i += blockDim.x) {
+      double v = F[i + (size_t)f * k];
+      const double* lr = Lp + (size_t)(i - r0) * NB;
+      for (int j = 0; j < kw; j++) v -= lr[j] * wk[j];
+      wc0[i - r0] = v;
+      const double a = fabs(v);
+      if (i > k) {
+        if (i < ncand)
+          keep_larger(bv, bi, a, i);
+        else
+          cm = fmax(cm, a);
+      }
+    }
+    block_reduce(red, bv, bi, cm);
+    if (tid == 0) {
+      partA.v = bv;
+      partA.i = bi;
+      partA.m = cm;
+      partA.x = (k >= r0 && k < r1) ? wc0[k - r0] : 0.0;
+    }
+    cl.sync();  // B1: column partials visible
+
+    if (tid == 0) {
+      double gv = -1.0, gm = 0.0;
+      int gi = INT_MAX;
+      for (int r = 0; r < CL; r++) {
+        const Part* P = cl.map_shared_rank(&partA, r);
+        keep_larger(gv, gi, P->v, P->i);
+        gm = fmax(gm, P->m);
+      }
+      const double wkk = cl.map_shared_rank(&partA, ok)->x;
+      const bool has = (k + 1 < ncand);
+      const double abswkk = fabs(wkk);
+      const double abswik = has ? gv : 0.0;
+      const int imax = has ? (gi < ncand ? gi : k + 1) : k;
+      const double colmax = fmax(abswik, gm);
+      int step;
+      if (prm.cholesky) {
+        step = kOne;
+      } else if (root) {
+        if (fmax(abswkk, colmax) == 0.0)
+          step = kZero;
+        else if (abswkk >= alpha_bk * colmax)
+          step = kOne;
+        else
+          step = kNeedRow;
+      } else if (abswkk >= prm.pivot_tol && abswkk >= prm.ustab * colmax) {
+        step = kOne;
+      } else {
+        step = has ? kNeedRow : kDelay;
+      }
+      dec[0] = step;
+      dec[1] = imax;
+      dval[0] = wkk;
+      dval[1] = abswik;
+      dval[2] = colmax;
+    }
+    __syncthreads();
+    int step = dec[0];
+    int kpiv = k;
+    const int imax = dec[1];
+    if (step == kNeedRow) {
+      const int oi = imax / R;
+      if (tid < kw) wi[tid] = cl.map_shared_rank(Wp, oi)[(size_t)(imax - oi * R) * NB + tid];
+      __syncthreads();
+      double rm = 0.0, dummy = -1.0;
+      int di = INT_MAX;
+      for (int i = lo + tid; i < r1; i += blockDim.x) {
+        double v = (i < imax) ? F[imax + (size_t)f * i] : F[i + (size_t)f * imax];
+        const double* lr = Lp + (size_t)(i - r0) * NB;
+        for (int j = 0; j < kw; j++) v -= lr[j] * wi[j];
+        wc1[i - r0] = v;
+        if (i != imax) rm = fmax(rm, fabs(v));
+      }
+      block_reduce(red, dummy, di, rm);
+      if (tid == 0) {
+        partB.m = rm;
+        const bool own = (imax >= r0 && imax < r1);
+        partB.x = own ? wc1[imax - r0] : 0.0;
+        partB.y = own ? wc0[imax - r0] : 0.0;
+      }
+      cl.sync();  // B2: row partials visible
+      if (tid == 0) {
+        double rmax = 0.0;
+        for (int r = 0; r < CL; r++) rmax = fmax(rmax, cl.map_shared_rank(&partB, r)->m);
+        const Part* Po = cl.map_shared_rank(&partB, oi);
+        const double wii = Po->x;
+        const double wik = Po->y;
+        const double wkk = dval[0];
+        const double abswkk = fabs(wkk);
+        const double abswik = dval[1];
+        const double colmax = dval[2];
+        const double abswii = fabs(wii);
+        int st, kp = k;
+        if (root) {
+          if (abswkk >= alpha_bk * colmax * (colmax / rmax)) {
+            st = kOne;
+          } else if (abswii >= alpha_bk * rmax) {
+            st = kOne;
+            kp = imax;
+          } else {
+            st = kTwo;
+            kp = imax;
+          }
+        } else if (abswii >= prm.pivot_tol && abswii >= prm.ustab * rmax) {
+          st = kOne;
+          kp = imax;
+        } else {
+          const double det = fabs(wkk * wii - wik * wik);
+          st = kDelay;
+          if (det >= prm.pivot_tol) {
+            const double delta = det / fmax(abswii + abswik, abswkk + abswik);
+            if (delta >= prm.ustab * colmax && delta >= prm.ustab * rmax) {
+              st = kTwo;
+              kp = imax;
+            }
+          }
+        }
+        dec[0] = st;
+        dec[2] = kp;
+      }
+      __syncthreads();
+      step = dec[0];
+      kpiv = dec[2];
+    }
+
+    if (step == kDelay) {
+      if (k < ncand - 1)
+        cluster_swap<CL>(cl, rank, F, f, fv, orig, k, ncand - 1, R, NB, kw, Lp, Wp, wc0, wc1);
+      ncand -= 1;
+      cl.sync();  // B3: swap visible
+      continue;
+    }
+    const int nstep = (step == kTwo) ? 2 : 1;
+    const int ksrc = k + nstep - 1;
+    // the pivot columns: 1x1 at k -> wc0; 1x1 at imax -> wc1; 2x2 -> wc0, wc1
+    const bool use1 = (step != kTwo) && (kpiv != k);
+    if (kpiv != ksrc) {
+      cluster_swap<CL>(cl, rank, F, f, fv, orig, ksrc, kpiv, R, NB, kw, Lp, Wp, wc0, wc1);
+      cl.sync();  // B3
+    }
+    double* colA = use1 ? wc1 : wc0;
+    if (tid == 0) {
+      const int o0 = k / R;
+      dval[3] = cl.map_shared_rank(colA, o0)[k - o0 * R];
+      if (nstep == 2) {
+        const int o1 = (k + 1) / R;
+        dval[4] = cl.map_shared_rank(wc0, o1)[(k + 1) - o1 * R];
+        dval[5] = cl.map_shared_rank(wc1, o1)[(k + 1) - o1 * R];
+      }
+    }
+    __syncthreads();
+    if (nstep == 1) {
+      const double d = dval[3];
+      const bool zero = (step == kZero) || (root && d == 0.0);
+      const double dinv = zero ? 0.0 : 1.0 / d;
+      for (int i = lo + tid; i < r1; i += blockDim.x) {
+        const double w = colA[i - r0];
+        double* lr = Lp + (size_t)(i - r0) * NB;
+        double* wr = Wp + (size_t)(i - r0) * NB;
+        if (i == k) {
+          lr[kw] = d;
+          wr[kw] = d;
+          F[k + (size_t)f * k] = d;
+        } else {
+          const double l = w * dinv;
+          lr[kw] = l;
+          wr[kw] = w;
+          F[i + (size_t)f * k] = l;
+        }
+      }
+      if (rank == 0 && tid == 0) {
+        if (d >= 0.0)
+          npos++;
+        else
+          nneg++;
+        flops += 2.0 * (double)(f - k) * (kw + 1);
+      }
+    } else {
+      const double d11 = dval[3], d21 = dval[4], d22 = dval[5];
+      const double det = d11 * d22 - d21 * d21;
+      const double detinv = 1.0 / det;
+      const double i00 = d22 * detinv, i01 = -d21 * detinv, i11 = d11 * detinv;
+      for (int i = lo + tid; i < r1; i += blockDim.x) {
+        double* lr = Lp + (size_t)(i - r0) * NB;
+        double* wr = Wp + (size_t)(i - r0) * NB;
+        const double a = wc0[i - r0];
+        const double b = wc1[i - r0];
+        if (i == k) {
+          lr[kw] = d11;
+          lr[kw + 1] = 0.0;
+          wr[kw] = a;
+          wr[kw + 1] = b;
+          F[k + (size_t)f * k] = d11;
+        } else if (i == k + 1) {
+          lr[kw] = d21;
+          lr[kw + 1] = d22;
+          wr[kw] = a;
+          wr[kw + 1] = b;
+          F[k + 1 + (size_t)f * k] = d21;
+          F[k + 1 + (size_t)f * (k + 1)] = d22;
+        } else {
+          const double l0 = a * i00 + b * i01;
+          const double l1 = a * i01 + b * i11;
+          lr[kw] = l0;
+          lr[kw + 1] = l1;
+          wr[kw] = a;
+          wr[kw + 1] = b;
+          F[i + (size_t)f * k] = l0;
+          F[i + (size_t)f * (k + 1)] = l1;
+        }
+      }
+      if (rank == 0 && tid == 0) {
+        fv[k] = -(fv[k] + 1);
+        fv[k + 1] = -(fv[k + 1] + 1);
+        if (det >= 0.0) {
+          if (d11 >= 0.0)
+            npos += 2;
+          else
+            nneg += 2;
+        } else {
+          npos++;
+          nneg++;
+        }
+        flops += 4.0 * (double)(f - k) * (kw + 2);
+      }
+    }
+    k += nstep;
+    kw += nstep;
+    cl.sync();  // B4: new panel columns visible
+  }
+
+  // W columns of the panel for the trailing update (rows >= k)
+  for (int j = 0; j < kw; j++) {
+    const int lo2 = max(r0, k);
+    for (int i = lo2 + tid; i < r1; i += blockDim.x)
+      Wg[(size_t)j * f + i] = Wp[(size_t)(i - r0) * NB + j];
+  }
+  if (rank == 0 && tid == 0) {
+    B->k = k;
+    B->ncand = ncand;
+    B->kstart = kstart;
+    B->kw = kw;
+    B->npos += npos;
+    B->nneg += nneg;
+    B->flops += flops;
+    if (k >= ncand) B->state = 1;
+  }
+}
+
+// --------------------------------------------------------- trailing update
+
+__global__ void big_tiles_kernel(DevState s, int nbig) {
+  // one CTA: prefix sum of lower-triangular 64x64 tile counts
+  __shared__ long long carry;
+  if (threadIdx.x == 0) {
+    carry = 0;
+    s.tile_ptr[0] = 0;
+  }
+  __syncthreads();
+  for (int base = 0; base < nbig; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    long long cnt = 0;
+    if (i < nbig) {
+      const BigFront& B = s.big[i];
+      if (B.state != 2 && B.kw > 0) {
+        const long long t = (B.f - B.k + kTile - 1) / kTile;
+        cnt = t * (t + 1) / 2;
+      }
+    }
+    // inclusive scan in the block (simple, nbig is small)
+    __shared__ long long buf[1024];
+    buf[threadIdx.x] = cnt;
+    __syncthreads();
+    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+      long long v = (threadIdx.x >= (unsigned)o) ? buf[threadIdx.x - o] : 0;
+      __syncthreads();
+      buf[threadIdx.x] += v;
+      __syncthreads();
+    }
+    if (i < nbig) s.tile_ptr[i + 1] = carry + buf[threadIdx.x];
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry += buf[threadIdx.x];
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kUpdThreads) big_update_kernel(DevState s, int nbig) {
+  __shared__ double As[kBigPanelMax][kTile];
+  __shared__ double Bs[kBigPanelMax][kTile];
+  const long long total = s.tile_ptr[nbig];
+  const int tx = threadIdx.x & 15;
+  const int ty = threadIdx.x >> 4;
+  for (long long t = blockIdx.x; t < total; t += gridDim.x) {
+    // find the front: last fi with tile_ptr[fi] <= t
+    int lo = 0, hi = nbig;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (s.tile_ptr[mid] <= t)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const BigFront& B = s.big[lo];
+    const long long lt = t - s.tile_ptr[lo];
+    int I = (int)((sqrt(8.0 * (double)lt + 1.0) - 1.0) * 0.5);
+    while ((long long)(I + 1) * (I + 2) / 2 <= lt) I++;
+    while ((long long)I * (I + 1) / 2 > lt) I--;
+    const int J = (int)(lt - (long long)I * (I + 1) / 2);
+    const int f = B.f;
+    const int k = B.k;
+    const int kw = B.kw;
+    const int ks = B.kstart;
+    const double* F0 = s.dpool + B.doff;
+    double* F = s.dpool + B.doff;
+    const double* W = s.dpool + B.woff;
+    const int i0 = k + I * kTile;
+    const int j0 = k + J * kTile;
+    __syncthreads();
+    for (int q = threadIdx.x; q < kw * kTile; q += blockDim.x) {
+      const int c = q / kTile;
+      const int r = q - c * kTile;
+      const int i = i0 + r;
+      const int j = j0 + r;
+      As[c][r] = (i < f) ? F0[i + (size_t)f * (ks + c)] : 0.0;
+      Bs[c][r] = (j < f) ? W[(size_t)c * f + j] : 0.0;
+    }
+    __syncthreads();
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+    for (int c = 0; c < kw; c++) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int a = 0; a < 4; a++) av[a] = As[c][tx + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; b++) bv[b] = Bs[c][ty + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+    }
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const int j = j0 + ty + 16 * b;
+      if (j >= f) continue;
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const int i = i0 + tx + 16 * a;
+        if (i < f && i >= j) F[i + (size_t)f * j] -= acc[a][b];
+      }
+    }
+  }
+}
+
+__global__ void big_after_update_kernel(DevState s, int nbig) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nbig) return;
+  BigFront& B = s.big[i];
+  if (B.state == 2) return;
+  if (B.kw > 0) {
+    const double r = (double)(B.f - B.k);
+    B.flops += r * (r + 1.0) * B.kw;
+  }
+  B.kw = 0;
+  if (B.state == 1) B.state = 2;
+}
+
+__global__ void big_finalize_kernel(DevState s, int nbig, int cholesky) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nbig) return;
+  const BigFront& B = s.big[i];
+  const int node = B.node;
+  const int npiv = B.k;
+  const int m = B.f - npiv;
+  s.f[node] = B.f;
+  s.fs[node] = B.fs;
+  s.npiv[node] = npiv;
+  s.ndel[node] = B.fs - npiv;
+  s.fv_off[node] = B.ioff;
+  s.L_off[node] = B.doff;
+  s.L_ld[node] = B.f;
+  s.cb_off[node] = B.doff + (long long)npiv * (B.f + 1);
+  s.cb_ld[node] = B.f;
+  s.u_off[node] = (long long)atomicAdd(s.used + 2, (unsigned long long)m);
+  if (!cholesky) {
+    atomicAdd(s.inertia, B.npos);
+    atomicAdd(s.inertia + 1, B.nneg);
+  }
+  atomicAdd(s.flops, B.flops);
+}
+
+template <int CL>
+cudaError_t launch_panel(const DevState& s, const FactorParams& prm, int count, int NB,
+                         size_t smem, cudaStream_t stream) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(count * CL, 1, 1);
+  cfg.blockDim = dim3(kPanelThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, big_panel_kernel<CL>, s, prm, NB);
+}
+
+constexpr size_t kPanelSmemMax = 224 * 1024;
+
+}  // namespace
+
+cudaError_t configure_big_kernels() {
+  cudaError_t e;
+  e = cudaFuncSetAttribute(big_panel_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kPanelSmemMax);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(big_panel_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kPanelSmemMax);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(big_panel_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kPanelSmemMax);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(big_panel_kernel<16>,
+                              cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+
+cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
+                             int maxkids, const FactorParams& prm, const double* vals,
+                             const double* diag, cudaStream_t stream) {
+  const int nb = info.count;
+  if (nb <= 0) return cudaSuccess;
+  const int cols_per = 8;  // warps per CTA in the assembly kernels
+  const int ychunks = std::min(256, (info.max_f + cols_per - 1) / cols_per);
+  big_zero_kernel<<<dim3(nb, ychunks), 256, 0, stream>>>(s);
+  big_scatter_kernel<<<dim3(nb, 16), 256, 0, stream>>>(p, s, vals, diag);
+  if (diag) big_diag_kernel<<<nb, 256, 0, stream>>>(p, s, diag);
+  for (int c = 0; c < maxkids; c++)
+    big_extend_kernel<<<dim3(nb, ychunks), 256, 0, stream>>>(p, s, c);
+
+  // cluster size and panel width from the largest front of the level
+  int CL = info.max_f > 1536 ? 16 : (info.max_f > 512 ? 8 : 4);
+  const int R = (info.max_f + CL - 1) / CL;
+  int NB = kBigPanelMax;
+  while (NB > 4 && (size_t)R * (2 * NB + 2) * sizeof(double) > kPanelSmemMax) NB >>= 1;
+  const size_t smem = (size_t)R * (2 * NB + 2) * sizeof(double);
+  const int steps = (info.max_fs + (NB - 2)) / (NB - 1) + 1;
+  const int upd_grid = 148 * 4;
+  for (int st = 0; st < steps; st++) {
+    cudaError_t e;
+    if (CL == 16)
+      e = launch_panel<16>(s, prm, nb, NB, smem, stream);
+    else if (CL == 8)
+      e = launch_panel<8>(s, prm, nb, NB, smem, stream);
+    else
+      e = launch_panel<4>(s, prm, nb, NB, smem, stream);
+    if (e != cudaSuccess) return e;
+    big_tiles_kernel<<<1, 1024, 0, stream>>>(s, nb);
+    big_update_kernel<<<upd_grid, kUpdThreads, 0, stream>>>(s, nb);
+    big_after_update_kernel<<<(nb + 255) / 256, 256, 0, stream>>>(s, nb);
+  }
+  big_finalize_kernel<<<(nb + 255) / 256, 256, 0, stream>>>(s, nb, prm.cholesky);
+  return cudaGetLastError();
+}
+
+}  // namespace b200ldl

@@ -140,8 +140,8 @@ __global__ void __launch_bounds__(kFactorThreads)
     if (io + 2ull * f > s.icap) fail = 1;
     sh_ioff = (long long)io;
     if (big) {
-      // the front itself plus two saved columns
-      const unsigned long long need = (unsigned long long)f * f + 2ull * f;
+      // the front itself plus the panel's W columns
+      const unsigned long long need = (unsigned long long)f * f + (unsigned long long)kBigPanelMax * f;
       const unsigned long long dofs = atomicAdd(s.used + 1, need);
       if (dofs + need > s.dcap) fail = 1;
       sh_doff = (long long)dofs;
@@ -157,6 +157,48 @@ __global__ void __launch_bounds__(kFactorThreads)
 
   int* fv = s.ivars + sh_ioff;
   int* orig = fv + f;
+  if (big) {
+    // front variables now; assembly and factorization by the big-front kernels
+    const int v0b = p.var_ptr[node];
+    for (int t = tid; t < ns; t += blockDim.x) fv[t] = p.node_to_var[v0b + t];
+    int offb = ns;
+    for (int c = kb; c < ke; c++) {
+      const int ch = p.kids[c];
+      const int nd = s.ndel[ch];
+      const int* cfv = s.ivars + s.fv_off[ch] + s.npiv[ch];
+      for (int t = tid; t < nd; t += blockDim.x) fv[offb + t] = cfv[t];
+      offb += nd;
+    }
+    const int cb0 = p.cptr[node];
+    for (int t = tid; t < nc; t += blockDim.x) fv[fs + t] = p.contrib_rows[cb0 + t];
+    for (int t = tid; t < f; t += blockDim.x) orig[t] = t;
+    if (tid == 0) {
+      const int slot = atomicAdd(s.big_meta, 1);
+      atomicMax(s.big_meta + 1, f);
+      atomicMax(s.big_meta + 2, fs);
+      BigFront b;
+      b.node = node;
+      b.f = f;
+      b.fs = fs;
+      b.ns = ns;
+      b.nd_in = nd_in;
+      b.nc = nc;
+      b.k = 0;
+      b.ncand = fs;
+      b.kstart = 0;
+      b.kw = 0;
+      b.state = 0;
+      b.npos = 0;
+      b.nneg = 0;
+      b.pad = 0;
+      b.ioff = sh_ioff;
+      b.doff = sh_doff;
+      b.woff = sh_doff + (long long)f * f;
+      b.flops = 0.0;
+      s.big[slot] = b;
+    }
+    return;
+  }
   double* F;
   int ld;
   if (big) {
@@ -278,7 +320,9 @@ __global__ void __launch_bounds__(kFactorThreads)
       const double abswkk = fabs(wkk);
       const bool has_cand = (k + 1 < ncand);
       const double abswik = has_cand ? bv : 0.0;
-      const int imax = has_cand ? bi : k;
+      // bi stays INT_MAX only if every candidate entry is NaN; keep imax a
+      // valid candidate index so the rest of the step stays in bounds
+      const int imax = has_cand ? (bi < ncand ? bi : k + 1) : k;
       const double colmax = fmax(abswik, cmx);
       if (root) {
         if (fmax(abswkk, colmax) == 0.0) {

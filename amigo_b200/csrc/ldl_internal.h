@@ -28,6 +28,22 @@ struct DevPlan {
   const int* scat_col;      // own column j
 };
 
+// A front too large for shared memory, registered by the level kernel and
+// factored by the cluster panel / tiled update kernels.
+struct BigFront {
+  int node, f, fs, ns, nd_in, nc;
+  int k, ncand, kstart, kw;
+  int state;  // 0 active, 1 finished after the pending update, 2 done
+  int npos, nneg;
+  int pad;
+  long long ioff;  // front variables (fv[f], orig[f]) in the int pool
+  long long doff;  // the front F (f x f, column-major) in the double pool
+  long long woff;  // the panel's W columns (f x kBigPanelMax) in the double pool
+  double flops;
+};
+
+constexpr int kBigPanelMax = 32;
+
 // Mutable state of one factorization (device memory).
 struct DevState {
   int* f;       // [nn] front size at run time
@@ -47,6 +63,9 @@ struct DevState {
   int* err;         // [4]: [0] overflow flag, [1] node of first error
   int* inertia;     // [2] pos, neg
   double* flops;    // [1] executed factor flops (accumulated)
+  BigFront* big;    // [nn] big fronts of the current level
+  int* big_meta;    // [4]: count, max f, max fs, unused
+  long long* tile_ptr;  // [nn+1] update tiles per big front (prefix)
 };
 
 struct FactorParams {
@@ -65,6 +84,16 @@ void launch_factor_level(const DevPlan& p, const DevState& s,
                          const double* vals, const double* diag);
 cudaError_t configure_factor_kernels();
 size_t factor_smem_bytes();
+
+// Big-front pipeline for one level (see big.cu). `maxkids` is the largest
+// number of children among the level's supernodes.
+struct BigLevelInfo {
+  int count, max_f, max_fs;
+};
+cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
+                      int maxkids, const FactorParams& prm, const double* vals,
+                      const double* diag, cudaStream_t stream);
+cudaError_t configure_big_kernels();
 
 constexpr int kSolveThreads = 256;
 // Front vectors of the solve live in shared memory up to this front size.

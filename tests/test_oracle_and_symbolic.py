@@ -1,0 +1,125 @@
+"""CPU tests: the oracle pinned against the reference's golden cases, the
+C-ABI library's exported symbols, and the host symbolic phase compared
+bit-for-bit with the reference's (ordering, supernode partition, children,
+contribution rows)."""
+
+import os
+import re
+
+import numpy as np
+import pytest
+
+from amigo_b200 import _native
+from amigo_b200.sparse_ldl import CSRMat, OrderingType, SparseLDL
+from amigo_b200.workloads import (batched_optimal_control, csr_from_coo,
+                                  optimal_control_kkt, plane_stress_kkt, poisson_2d)
+from oracle import ref
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_exports_every_declared_symbol():
+    header = open(os.path.join(ROOT, "include", "b200ldl.h")).read()
+    declared = set(re.findall(r"\b(b200ldl_[a-z_]+)\s*\(", header))
+    assert declared, "no declarations found"
+    lib = _native.load()
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert declared == set(_native.SIGNATURES)
+
+
+@pytest.mark.parametrize("order", ["natural", "amd"])
+def test_oracle_matches_reference_golden(golden, order):
+    """The compiled reference reproduces the reference tests' assertions
+    (tests/unit/test_ldl.py: exact inertia, 7-RHS solutions of A x = A 1 to
+    1e-11) and the stored fixture."""
+    code = ref.ORDER_NATURAL if order == "natural" else ref.ORDER_AMD
+    for name in golden["names"]:
+        rowp = golden[f"{name}/rowp"]
+        cols = golden[f"{name}/cols"]
+        vals = golden[f"{name}/vals"]
+        r = ref.RefLDL(rowp, cols, order=code, ustab=0.4)
+        assert r.factor(vals) == 0
+        assert tuple(r.inertia()) == tuple(golden[f"{name}/inertia"]), name
+        assert tuple(r.inertia()) == tuple(golden[f"{name}/{order}/inertia"]), name
+        X = np.tile(golden[f"{name}/rhs"][:, None], (1, 7))
+        x = r.solve(X)
+        assert np.abs(x - golden[f"{name}/x"][:, None]).max() < 1e-11, name
+        assert np.abs(x - golden[f"{name}/{order}/solution"]).max() < 1e-13, name
+
+
+def _compare_symbolic(rowp, cols, order):
+    n = len(rowp) - 1
+    mine = SparseLDL(CSRMat(n, n, rowp, cols), order=order)
+    theirs = ref.RefLDL(rowp, cols, order=int(order))
+    a = mine.symbolic()
+    b = theirs.symbolic()
+    for key in a:
+        assert a[key].shape == b[key].shape, key
+        assert np.array_equal(a[key], b[key]), key
+
+
+@pytest.mark.parametrize("order", [OrderingType.AMD, OrderingType.NATURAL,
+                                   OrderingType.NESTED_DISSECTION])
+def test_symbolic_matches_reference_golden_cases(golden, order):
+    for name in golden["names"]:
+        _compare_symbolic(golden[f"{name}/rowp"], golden[f"{name}/cols"], order)
+
+
+@pytest.mark.parametrize("order", [OrderingType.AMD, OrderingType.NATURAL])
+def test_symbolic_matches_reference_kkt(order):
+    s = optimal_control_kkt()
+    _compare_symbolic(s.rowp, s.cols, order)
+    for s in batched_optimal_control(num_systems=6, seed=3):
+        _compare_symbolic(s.rowp, s.cols, order)
+    for nel in (4, 16, 48):
+        s = plane_stress_kkt(nel)
+        _compare_symbolic(s.rowp, s.cols, order)
+
+
+def test_symbolic_matches_reference_random_patterns():
+    rng = np.random.default_rng(7)
+    for _ in range(40):
+        n = int(rng.integers(1, 250))
+        dens = rng.random() * 0.08
+        a = rng.random((n, n)) < dens
+        a = a | a.T
+        r, c = np.nonzero(a)
+        rowp, cols, _ = csr_from_coo(n, r, c, np.ones(len(r)))
+        _compare_symbolic(rowp, cols, OrderingType.AMD)
+
+
+def test_symbolic_handles_disconnected_and_trivial():
+    # n = 1, diagonal only, and a block-diagonal (forest) pattern
+    for n, r, c in ((1, [0], [0]), (5, list(range(5)), list(range(5))),
+                    (6, [0, 1, 3, 4], [1, 0, 4, 3])):
+        rowp, cols, _ = csr_from_coo(n, r, c, np.ones(len(r)))
+        _compare_symbolic(rowp, cols, OrderingType.AMD)
+        _compare_symbolic(rowp, cols, OrderingType.NATURAL)
+
+
+@pytest.mark.slow
+def test_symbolic_matches_reference_plane_stress_256():
+    s = plane_stress_kkt(256)
+    _compare_symbolic(s.rowp, s.cols, OrderingType.AMD)
+
+
+def test_create_rejects_bad_input():
+    with pytest.raises(_native.NativeError):
+        SparseLDL(CSRMat(2, 2, [0, 1, 2], [0, 5], [1.0, 1.0]))
+    with pytest.raises(_native.NativeError):
+        SparseLDL(CSRMat(2, 2, [0, 1, 2], [0, 1], [1.0, 1.0]), order=OrderingType.MULTI_COLOR)
+
+
+def test_poisson_generator_matches_reference_matrix(golden):
+    for n in (10, 20, 50):
+        rowp, cols, vals = poisson_2d(n)
+        m = (n - 1) ** 2
+        a = np.zeros((m, m))
+        r = np.repeat(np.arange(m), np.diff(rowp))
+        a[r, cols] = vals
+        g = np.zeros((m, m))
+        gr = golden[f"poisson{n}/rowp"]
+        g[np.repeat(np.arange(m), np.diff(gr)), golden[f"poisson{n}/cols"]] = \
+            golden[f"poisson{n}/vals"]
+        assert np.array_equal(a, g)
