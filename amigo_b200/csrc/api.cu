@@ -109,6 +109,9 @@ struct b200ldl_handle {
   unsigned long long used[3] = {0, 0, 0};
   double exec_flops = 0.0;
   int fmax = 0;
+  std::vector<int> level_fmax;
+  Prof prof;
+  double flops4[4] = {0, 0, 0, 0};
   double sum_delayed = 0.0;
 };
 
@@ -300,10 +303,10 @@ void upload_plan(b200ldl_t h) {
   CK(h->d_u_off.alloc(nn));
   CK(h->d_err.alloc(4));
   CK(h->d_inertia.alloc(2));
-  CK(h->d_flops.alloc(1));
+  CK(h->d_flops.alloc(4));
   CK(h->d_used.alloc(3));
   CK(h->d_big.alloc(nn));
-  CK(h->d_big_meta.alloc(4));
+  CK(h->d_big_meta.alloc(8));
   CK(h->d_tile_ptr.alloc(nn + 1));
   h->uploaded = true;
 }
@@ -355,23 +358,25 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
     CK(cudaMemsetAsync(h->d_err.ptr, 0, sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_err.ptr + 1, 0xff, sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_inertia.ptr, 0, 2 * sizeof(int), h->stream));
-    CK(cudaMemsetAsync(h->d_flops.ptr, 0, sizeof(double), h->stream));
+    CK(cudaMemsetAsync(h->d_flops.ptr, 0, 4 * sizeof(double), h->stream));
     CK(cudaMemsetAsync(h->d_ndel.ptr, 0, sizeof(int) * std::max(1, h->sym.num_nodes), h->stream));
     for (int l = 0; l < h->num_levels; l++) {
       const int b = h->level_ptr[l];
       const int cnt = h->level_ptr[l + 1] - b;
-      CK(cudaMemsetAsync(h->d_big_meta.ptr, 0, 4 * sizeof(int), h->stream));
+      CK(cudaMemsetAsync(h->d_big_meta.ptr, 0, 8 * sizeof(int), h->stream));
+      h->prof.begin(h->stream);
       launch_factor_level(h->plan, h->st, h->d_level_nodes.ptr + b, cnt, prm, h->stream,
                           vals, diag);
+      h->prof.end(kPhFront, h->stream, 1);
       CK(cudaGetLastError());
-      int meta[4];
-      CK(cudaMemcpyAsync(meta, h->d_big_meta.ptr, 4 * sizeof(int), cudaMemcpyDeviceToHost,
+      int meta[8];
+      CK(cudaMemcpyAsync(meta, h->d_big_meta.ptr, 8 * sizeof(int), cudaMemcpyDeviceToHost,
                          h->stream));
       CK(cudaStreamSynchronize(h->stream));
       if (meta[0] > 0) {
-        BigLevelInfo info{meta[0], meta[1], meta[2]};
+        BigLevelInfo info{meta[0], meta[1], meta[2], meta[3], meta[4], meta[5]};
         CK(launch_big_level(h->plan, h->st, info, h->level_maxkids[l], prm, vals, diag,
-                            h->stream));
+                            h->stream, h->prof));
       }
     }
     CK(cudaGetLastError());
@@ -381,9 +386,11 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
                        cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(h->inertia, h->d_inertia.ptr, 2 * sizeof(int), cudaMemcpyDeviceToHost,
                        h->stream));
-    CK(cudaMemcpyAsync(&h->exec_flops, h->d_flops.ptr, sizeof(double), cudaMemcpyDeviceToHost,
+    CK(cudaMemcpyAsync(h->flops4, h->d_flops.ptr, 4 * sizeof(double), cudaMemcpyDeviceToHost,
                        h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    h->exec_flops = h->flops4[0];
+    h->prof.collect();
     if (err[0] == 0) {
       h->factored = true;
       return;
@@ -396,30 +403,43 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
   throw std::runtime_error("factor storage did not converge after repeated growth");
 }
 
-int max_front(b200ldl_t h) {
+
+// largest front of every level of the last factorization
+void level_fronts(b200ldl_t h) {
   const int nn = h->sym.num_nodes;
   std::vector<int> f(nn);
   CK(cudaMemcpy(f.data(), h->d_f.ptr, nn * sizeof(int), cudaMemcpyDeviceToHost));
+  h->level_fmax.assign(h->num_levels, 1);
   int m = 1;
-  for (int v : f) m = std::max(m, v);
-  return m;
+  for (int l = 0; l < h->num_levels; l++) {
+    for (int q = h->level_ptr[l]; q < h->level_ptr[l + 1]; q++)
+      h->level_fmax[l] = std::max(h->level_fmax[l], f[h->hp_level_nodes[q]]);
+    m = std::max(m, h->level_fmax[l]);
+  }
+  h->fmax = m;
 }
 
 void run_solve(b200ldl_t h, int nrhs, double* x, int ldx) {
-  if (h->fmax == 0) h->fmax = max_front(h);
-  if (h->fmax > kSolveSmemFront)
+  if (h->fmax == 0) level_fronts(h);
+  if (solve_rhs_chunk(h->fmax, 1) < 1)
     throw std::runtime_error("front too large for the solve kernels");
   const size_t need = (size_t)h->used[2] * nrhs;
   if (h->d_upool.count < need) CK(h->d_upool.alloc(need));
   for (int l = 0; l < h->num_levels; l++) {
     const int b = h->level_ptr[l];
-    launch_forward_level(h->plan, h->st, h->d_level_nodes.ptr + b, h->level_ptr[l + 1] - b, x,
-                         ldx, nrhs, h->d_upool.ptr, h->fmax, h->stream);
+    h->prof.begin(h->stream);
+    const int nl = launch_forward_level(h->plan, h->st, h->d_level_nodes.ptr + b,
+                                        h->level_ptr[l + 1] - b, x, ldx, nrhs, h->d_upool.ptr,
+                                        h->level_fmax[l], h->stream);
+    h->prof.end(kPhFwd, h->stream, nl);
   }
   for (int l = h->num_levels - 1; l >= 0; l--) {
     const int b = h->level_ptr[l];
-    launch_backward_level(h->plan, h->st, h->d_level_nodes.ptr + b, h->level_ptr[l + 1] - b, x,
-                          ldx, nrhs, h->fmax, h->stream);
+    h->prof.begin(h->stream);
+    const int nl = launch_backward_level(h->plan, h->st, h->d_level_nodes.ptr + b,
+                                         h->level_ptr[l + 1] - b, x, ldx, nrhs,
+                                         h->level_fmax[l], h->stream);
+    h->prof.end(kPhBwd, h->stream, nl);
   }
   CK(cudaGetLastError());
 }
@@ -523,6 +543,7 @@ int b200ldl_solve(b200ldl_t h, int nrhs, double* x, int ldx) {
     if (nrhs == 0 || h->n == 0) return 0;
     run_solve(h, nrhs, x, ldx);
     CK(cudaStreamSynchronize(h->stream));
+    h->prof.collect();
     return 0;
   });
 }
@@ -538,6 +559,7 @@ int b200ldl_solve_host(b200ldl_t h, int nrhs, double* x, int ldx) {
     run_solve(h, nrhs, h->d_x.ptr, ldx);
     CK(cudaMemcpyAsync(x, h->d_x.ptr, cnt * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    h->prof.collect();
     return 0;
   });
 }
@@ -609,6 +631,35 @@ int b200ldl_stats(b200ldl_t h, double* stats, int nstats) {
     for (int i = 0; i < nstats && i < 6; i++) stats[i] = v[i];
     return 0;
   });
+}
+
+int b200ldl_set_profiling(b200ldl_t h, int enable) {
+  if (!h) return -1;
+  h->prof.on = enable != 0;
+  return 0;
+}
+
+int b200ldl_reset_profile(b200ldl_t h) {
+  if (!h) return -1;
+  h->prof.reset();
+  return 0;
+}
+
+int b200ldl_profile(b200ldl_t h, double* out, int n) {
+  if (!h || !out) return -1;
+  for (int p = 0; p < kPhN && 2 * p + 1 < n; p++) {
+    out[2 * p] = h->prof.ms[p];
+    out[2 * p + 1] = (double)h->prof.launches[p];
+  }
+  return 0;
+}
+
+long long b200ldl_launch_count(b200ldl_t h) { return h ? h->prof.total_launches : -1; }
+
+int b200ldl_work(b200ldl_t h, double* out, int n) {
+  if (!h || !out) return -1;
+  for (int i = 0; i < 4 && i < n; i++) out[i] = h->flops4[i];
+  return 0;
 }
 
 }  // extern "C"

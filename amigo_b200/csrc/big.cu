@@ -175,10 +175,10 @@ __global__ void big_extend_kernel(DevPlan p, DevState s, int c) {
 // Symmetric interchange of rows/columns a < b: the front in global memory
 // (all CTAs of the cluster share the element range), the panel rows held in
 // shared memory (exchanged by the owner of row a through DSMEM), and the
-// front-variable / original-position lists.
+// front-variable / original-position lists. The caller barriers afterwards.
 template <int CL>
 __device__ void cluster_swap(cg::cluster_group& cl, int rank, double* F, int f, int* fv,
-                             int* orig, int a, int b, int R, int NB, int kw, double* Lp,
+                             int* orig, int a, int b, int R, int NBP, int kw, double* Lp,
                              double* Wp, double* wc0, double* wc1) {
   const int n1 = a;
   const int n2 = b - a - 1;
@@ -208,10 +208,10 @@ __device__ void cluster_swap(cg::cluster_group& cl, int rank, double* F, int f, 
   const int oa = a / R;
   const int ob = b / R;
   if (rank == oa) {
-    double* La = Lp + (size_t)(a - oa * R) * NB;
-    double* Wa = Wp + (size_t)(a - oa * R) * NB;
-    double* Lb = cl.map_shared_rank(Lp, ob) + (size_t)(b - ob * R) * NB;
-    double* Wb = cl.map_shared_rank(Wp, ob) + (size_t)(b - ob * R) * NB;
+    double* La = Lp + (size_t)(a - oa * R) * NBP;
+    double* Wa = Wp + (size_t)(a - oa * R) * NBP;
+    double* Lb = cl.map_shared_rank(Lp, ob) + (size_t)(b - ob * R) * NBP;
+    double* Wb = cl.map_shared_rank(Wp, ob) + (size_t)(b - ob * R) * NBP;
     for (int j = threadIdx.x; j < kw; j += blockDim.x) {
       double t = La[j];
       La[j] = Lb[j];
@@ -220,7 +220,7 @@ __device__ void cluster_swap(cg::cluster_group& cl, int rank, double* F, int f, 
       Wa[j] = Wb[j];
       Wb[j] = t;
     }
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 32) {
       double* x0 = cl.map_shared_rank(wc0, ob) + (b - ob * R);
       double* x1 = cl.map_shared_rank(wc1, ob) + (b - ob * R);
       double t = wc0[a - oa * R];
@@ -231,7 +231,7 @@ __device__ void cluster_swap(cg::cluster_group& cl, int rank, double* F, int f, 
       *x1 = t;
     }
   }
-  if (rank == 0 && threadIdx.x == 0) {
+  if (rank == 0 && threadIdx.x == 64) {
     int t = fv[a];
     fv[a] = fv[b];
     fv[b] = t;
@@ -243,54 +243,79 @@ __device__ void cluster_swap(cg::cluster_group& cl, int rank, double* F, int f, 
 
 enum : int { kDelay = 0, kOne = 1, kTwo = 2, kNeedRow = 3, kZero = 4 };
 
+// Partials are pushed: every CTA stores its partial into slot[rank] of every
+// CTA of the cluster (lanes of warp 0 in parallel), then one cluster barrier,
+// then every thread reduces its own CTA's slots. All CTAs reduce the same
+// values in the same order, so every thread of the cluster reaches the same
+// pivot decision and the same sequence of barriers.
 template <int CL>
+__device__ __forceinline__ void push_part(cg::cluster_group& cl, Part* slots, int rank,
+                                          const Part& p) {
+  if (threadIdx.x < CL) *cl.map_shared_rank(slots + rank, (unsigned)threadIdx.x) = p;
+}
+
+// FUSED (with CL == 1): one CTA factors a medium front completely in one
+// launch, alternating panels (in shared memory) and its own trailing update
+// from those panels. Otherwise one panel per launch, the trailing update
+// follows in big_update_kernel.
+template <int CL, bool FUSED>
 __global__ void __launch_bounds__(kPanelThreads)
-    big_panel_kernel(DevState s, FactorParams prm, int NB) {
+    big_panel_kernel(DevState s, FactorParams prm, int NB_arg, int smem_bytes) {
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
   BigFront* B = s.big + blockIdx.x / CL;
   extern __shared__ __align__(16) double sm[];
-  __shared__ Part partA, partB;
+  __shared__ Part slotA[CL], slotB[CL];
   __shared__ BlockRed red;
   __shared__ double wk[kBigPanelMax], wi[kBigPanelMax];
-  __shared__ int dec[4];
-  __shared__ double dval[8];
 
   const int tid = threadIdx.x;
   if (B->state != 0) return;  // same value in every CTA of the cluster
   const int f = B->f;
+  if (FUSED != (f <= kMediumMax)) return;  // the other path owns this front
+  int NB = NB_arg;
+  if (FUSED) {
+    // widest panel whose rows fit in the launch's shared memory
+    NB = kBigPanelMax;
+    while (NB > 4 && (size_t)f * (2 * (NB + 1) + 2) * sizeof(double) > (size_t)smem_bytes)
+      NB >>= 1;
+  }
   const bool root = (B->nc == 0);
   int k = B->k;
   int ncand = B->ncand;
+  const int NBP = NB + 1;  // odd row stride: conflict-free column access
   const int R = (f + CL - 1) / CL;
   const int r0 = rank * R;
   const int r1 = min(f, r0 + R);
   double* Lp = sm;
-  double* Wp = Lp + (size_t)R * NB;
-  double* wc0 = Wp + (size_t)R * NB;
+  double* Wp = Lp + (size_t)R * NBP;
+  double* wc0 = Wp + (size_t)R * NBP;
   double* wc1 = wc0 + R;
   double* F = s.dpool + B->doff;
   double* Wg = s.dpool + B->woff;
   int* fv = s.ivars + B->ioff;
   int* orig = fv + f;
   const double alpha_bk = (1.0 + 4.1231056256176605) / 8.0;  // (1 + sqrt(17)) / 8
-  const int kstart = k;
+  int kstart = k;
   int kw = 0;
   int npos = 0, nneg = 0;
-  double flops = 0.0;
+  double flops = 0.0, uflops = 0.0;
 
+  for (;;) {  // panels (more than one only when FUSED)
+  kstart = k;
+  kw = 0;
   while (kw < NB - 1 && k < ncand) {
     const int ok = k / R;
-    if (tid < kw) wk[tid] = cl.map_shared_rank(Wp, ok)[(size_t)(k - ok * R) * NB + tid];
+    if (tid < kw) wk[tid] = cl.map_shared_rank(Wp, ok)[(size_t)(k - ok * R) * NBP + tid];
     __syncthreads();
-    // candidate column k on this CTA's rows
+    // candidate column k on this CTA's rows: F(:,k) - Lp W(k,:)^T
     double bv = -1.0, cm = 0.0;
     int bi = INT_MAX;
     const int lo = max(r0, k);
     for (int i = lo + tid; i < r1; i += blockDim.x) {
       double v = F[i + (size_t)f * k];
-      const double* lr = Lp + (size_t)(i - r0) * NB;
-      for (int j = 0; j < kw; j++) v -= lr[j] * wk[j];
+      const double* lr = Lp + (size_t)(i - r0) * NBP;
+      for (int j = 0; j < kw; j++) v = fma(-lr[j], wk[j], v);
       wc0[i - r0] = v;
       const double a = fabs(v);
       if (i > k) {
@@ -301,121 +326,110 @@ __global__ void __launch_bounds__(kPanelThreads)
       }
     }
     block_reduce(red, bv, bi, cm);
-    if (tid == 0) {
-      partA.v = bv;
-      partA.i = bi;
-      partA.m = cm;
-      partA.x = (k >= r0 && k < r1) ? wc0[k - r0] : 0.0;
+    {
+      Part P;
+      P.v = bv;
+      P.i = bi;
+      P.pad = 0;
+      P.m = cm;
+      P.x = (k >= r0 && k < r1) ? wc0[k - r0] : 0.0;
+      P.y = 0.0;
+      push_part<CL>(cl, slotA, rank, P);
     }
     cl.sync();  // B1: column partials visible
 
-    if (tid == 0) {
-      double gv = -1.0, gm = 0.0;
-      int gi = INT_MAX;
-      for (int r = 0; r < CL; r++) {
-        const Part* P = cl.map_shared_rank(&partA, r);
-        keep_larger(gv, gi, P->v, P->i);
-        gm = fmax(gm, P->m);
-      }
-      const double wkk = cl.map_shared_rank(&partA, ok)->x;
-      const bool has = (k + 1 < ncand);
-      const double abswkk = fabs(wkk);
-      const double abswik = has ? gv : 0.0;
-      const int imax = has ? (gi < ncand ? gi : k + 1) : k;
-      const double colmax = fmax(abswik, gm);
-      int step;
-      if (prm.cholesky) {
-        step = kOne;
-      } else if (root) {
-        if (fmax(abswkk, colmax) == 0.0)
-          step = kZero;
-        else if (abswkk >= alpha_bk * colmax)
-          step = kOne;
-        else
-          step = kNeedRow;
-      } else if (abswkk >= prm.pivot_tol && abswkk >= prm.ustab * colmax) {
-        step = kOne;
-      } else {
-        step = has ? kNeedRow : kDelay;
-      }
-      dec[0] = step;
-      dec[1] = imax;
-      dval[0] = wkk;
-      dval[1] = abswik;
-      dval[2] = colmax;
+    double gv = -1.0, gm = 0.0;
+    int gi = INT_MAX;
+#pragma unroll
+    for (int r = 0; r < CL; r++) {
+      keep_larger(gv, gi, slotA[r].v, slotA[r].i);
+      gm = fmax(gm, slotA[r].m);
     }
-    __syncthreads();
-    int step = dec[0];
+    const double wkk = slotA[ok].x;
+    const bool has = (k + 1 < ncand);
+    const double abswkk = fabs(wkk);
+    const double abswik = has ? gv : 0.0;
+    const int imax = has ? (gi < ncand ? gi : k + 1) : k;
+    const double colmax = fmax(abswik, gm);
+    int step;
     int kpiv = k;
-    const int imax = dec[1];
+    if (prm.cholesky) {
+      step = kOne;
+    } else if (root) {
+      if (fmax(abswkk, colmax) == 0.0)
+        step = kZero;
+      else if (abswkk >= alpha_bk * colmax)
+        step = kOne;
+      else
+        step = kNeedRow;
+    } else if (abswkk >= prm.pivot_tol && abswkk >= prm.ustab * colmax) {
+      step = kOne;
+    } else {
+      step = has ? kNeedRow : kDelay;
+    }
+    double wii = 0.0, wik = 0.0;
     if (step == kNeedRow) {
       const int oi = imax / R;
-      if (tid < kw) wi[tid] = cl.map_shared_rank(Wp, oi)[(size_t)(imax - oi * R) * NB + tid];
+      if (tid < kw) wi[tid] = cl.map_shared_rank(Wp, oi)[(size_t)(imax - oi * R) * NBP + tid];
       __syncthreads();
       double rm = 0.0, dummy = -1.0;
       int di = INT_MAX;
       for (int i = lo + tid; i < r1; i += blockDim.x) {
         double v = (i < imax) ? F[imax + (size_t)f * i] : F[i + (size_t)f * imax];
-        const double* lr = Lp + (size_t)(i - r0) * NB;
-        for (int j = 0; j < kw; j++) v -= lr[j] * wi[j];
+        const double* lr = Lp + (size_t)(i - r0) * NBP;
+        for (int j = 0; j < kw; j++) v = fma(-lr[j], wi[j], v);
         wc1[i - r0] = v;
         if (i != imax) rm = fmax(rm, fabs(v));
       }
       block_reduce(red, dummy, di, rm);
-      if (tid == 0) {
-        partB.m = rm;
+      {
+        Part P;
         const bool own = (imax >= r0 && imax < r1);
-        partB.x = own ? wc1[imax - r0] : 0.0;
-        partB.y = own ? wc0[imax - r0] : 0.0;
+        P.v = 0.0;
+        P.i = 0;
+        P.pad = 0;
+        P.m = rm;
+        P.x = own ? wc1[imax - r0] : 0.0;
+        P.y = own ? wc0[imax - r0] : 0.0;
+        push_part<CL>(cl, slotB, rank, P);
       }
       cl.sync();  // B2: row partials visible
-      if (tid == 0) {
-        double rmax = 0.0;
-        for (int r = 0; r < CL; r++) rmax = fmax(rmax, cl.map_shared_rank(&partB, r)->m);
-        const Part* Po = cl.map_shared_rank(&partB, oi);
-        const double wii = Po->x;
-        const double wik = Po->y;
-        const double wkk = dval[0];
-        const double abswkk = fabs(wkk);
-        const double abswik = dval[1];
-        const double colmax = dval[2];
-        const double abswii = fabs(wii);
-        int st, kp = k;
-        if (root) {
-          if (abswkk >= alpha_bk * colmax * (colmax / rmax)) {
-            st = kOne;
-          } else if (abswii >= alpha_bk * rmax) {
-            st = kOne;
-            kp = imax;
-          } else {
-            st = kTwo;
-            kp = imax;
-          }
-        } else if (abswii >= prm.pivot_tol && abswii >= prm.ustab * rmax) {
-          st = kOne;
-          kp = imax;
+      double rmax = 0.0;
+#pragma unroll
+      for (int r = 0; r < CL; r++) rmax = fmax(rmax, slotB[r].m);
+      wii = slotB[oi].x;
+      wik = slotB[oi].y;
+      const double abswii = fabs(wii);
+      if (root) {
+        if (abswkk >= alpha_bk * colmax * (colmax / rmax)) {
+          step = kOne;
+        } else if (abswii >= alpha_bk * rmax) {
+          step = kOne;
+          kpiv = imax;
         } else {
-          const double det = fabs(wkk * wii - wik * wik);
-          st = kDelay;
-          if (det >= prm.pivot_tol) {
-            const double delta = det / fmax(abswii + abswik, abswkk + abswik);
-            if (delta >= prm.ustab * colmax && delta >= prm.ustab * rmax) {
-              st = kTwo;
-              kp = imax;
-            }
+          step = kTwo;
+          kpiv = imax;
+        }
+      } else if (abswii >= prm.pivot_tol && abswii >= prm.ustab * rmax) {
+        step = kOne;
+        kpiv = imax;
+      } else {
+        const double det = fabs(wkk * wii - wik * wik);
+        step = kDelay;
+        if (det >= prm.pivot_tol) {
+          const double delta = det / fmax(abswii + abswik, abswkk + abswik);
+          if (delta >= prm.ustab * colmax && delta >= prm.ustab * rmax) {
+            step = kTwo;
+            kpiv = imax;
           }
         }
-        dec[0] = st;
-        dec[2] = kp;
       }
-      __syncthreads();
-      step = dec[0];
-      kpiv = dec[2];
     }
 
     if (step == kDelay) {
       if (k < ncand - 1)
-        cluster_swap<CL>(cl, rank, F, f, fv, orig, k, ncand - 1, R, NB, kw, Lp, Wp, wc0, wc1);
+        cluster_swap<CL>(cl, rank, F, f, fv, orig, k, ncand - 1, R, NBP, kw, Lp, Wp, wc0,
+                         wc1);
       ncand -= 1;
       cl.sync();  // B3: swap visible
       continue;
@@ -425,28 +439,19 @@ __global__ void __launch_bounds__(kPanelThreads)
     // the pivot columns: 1x1 at k -> wc0; 1x1 at imax -> wc1; 2x2 -> wc0, wc1
     const bool use1 = (step != kTwo) && (kpiv != k);
     if (kpiv != ksrc) {
-      cluster_swap<CL>(cl, rank, F, f, fv, orig, ksrc, kpiv, R, NB, kw, Lp, Wp, wc0, wc1);
+      cluster_swap<CL>(cl, rank, F, f, fv, orig, ksrc, kpiv, R, NBP, kw, Lp, Wp, wc0, wc1);
       cl.sync();  // B3
     }
-    double* colA = use1 ? wc1 : wc0;
-    if (tid == 0) {
-      const int o0 = k / R;
-      dval[3] = cl.map_shared_rank(colA, o0)[k - o0 * R];
-      if (nstep == 2) {
-        const int o1 = (k + 1) / R;
-        dval[4] = cl.map_shared_rank(wc0, o1)[(k + 1) - o1 * R];
-        dval[5] = cl.map_shared_rank(wc1, o1)[(k + 1) - o1 * R];
-      }
-    }
-    __syncthreads();
+    const double* colA = use1 ? wc1 : wc0;
     if (nstep == 1) {
-      const double d = dval[3];
+      // pivot value known from the reduced partials: wkk (at k) or wii (at imax)
+      const double d = use1 ? wii : wkk;
       const bool zero = (step == kZero) || (root && d == 0.0);
       const double dinv = zero ? 0.0 : 1.0 / d;
       for (int i = lo + tid; i < r1; i += blockDim.x) {
         const double w = colA[i - r0];
-        double* lr = Lp + (size_t)(i - r0) * NB;
-        double* wr = Wp + (size_t)(i - r0) * NB;
+        double* lr = Lp + (size_t)(i - r0) * NBP;
+        double* wr = Wp + (size_t)(i - r0) * NBP;
         if (i == k) {
           lr[kw] = d;
           wr[kw] = d;
@@ -466,13 +471,14 @@ __global__ void __launch_bounds__(kPanelThreads)
         flops += 2.0 * (double)(f - k) * (kw + 1);
       }
     } else {
-      const double d11 = dval[3], d21 = dval[4], d22 = dval[5];
+      // 2x2 at (k, k+1) after moving imax to k+1: D = [wkk wik; wik wii]
+      const double d11 = wkk, d21 = wik, d22 = wii;
       const double det = d11 * d22 - d21 * d21;
       const double detinv = 1.0 / det;
       const double i00 = d22 * detinv, i01 = -d21 * detinv, i11 = d11 * detinv;
       for (int i = lo + tid; i < r1; i += blockDim.x) {
-        double* lr = Lp + (size_t)(i - r0) * NB;
-        double* wr = Wp + (size_t)(i - r0) * NB;
+        double* lr = Lp + (size_t)(i - r0) * NBP;
+        double* wr = Wp + (size_t)(i - r0) * NBP;
         const double a = wc0[i - r0];
         const double b = wc1[i - r0];
         if (i == k) {
@@ -519,21 +525,56 @@ __global__ void __launch_bounds__(kPanelThreads)
     cl.sync();  // B4: new panel columns visible
   }
 
-  // W columns of the panel for the trailing update (rows >= k)
-  for (int j = 0; j < kw; j++) {
-    const int lo2 = max(r0, k);
-    for (int i = lo2 + tid; i < r1; i += blockDim.x)
-      Wg[(size_t)j * f + i] = Wp[(size_t)(i - r0) * NB + j];
+  if constexpr (FUSED) {
+    // trailing update F(i,j) -= sum_c Lp(i,c) Wp(j,c), k <= j <= i < f, by
+    // this CTA with both panels in shared memory
+    if (kw > 0) {
+      __syncthreads();
+      const int lane = tid & 31;
+      const int warp = tid >> 5;
+      for (int j = k + warp; j < f; j += kPWarps) {
+        const double* wj = Wp + (size_t)j * NBP;
+        double* Fj = F + (size_t)f * j;
+        for (int i = j + lane; i < f; i += 32) {
+          const double* li = Lp + (size_t)i * NBP;
+          double acc = 0.0;
+          for (int c = 0; c < kw; c++) acc = fma(li[c], wj[c], acc);
+          Fj[i] -= acc;
+        }
+      }
+      if (tid == 0) {
+        const double r = (double)(f - k);
+        const double fl = r * (r + 1.0) * kw;
+        uflops += fl;
+        atomicAdd(s.flops + 2, fl);
+        atomicAdd(s.flops + 3, 8.0 * r * (r + 1.0));
+      }
+      __syncthreads();
+    }
+    if (k < ncand) continue;
+  } else {
+    // W columns of the panel for the trailing update (rows >= k)
+    for (int j = 0; j < kw; j++) {
+      const int lo2 = max(r0, k);
+      for (int i = lo2 + tid; i < r1; i += blockDim.x)
+        Wg[(size_t)j * f + i] = Wp[(size_t)(i - r0) * NBP + j];
+    }
   }
+  break;
+  }  // panels
   if (rank == 0 && tid == 0) {
     B->k = k;
     B->ncand = ncand;
     B->kstart = kstart;
-    B->kw = kw;
+    B->kw = FUSED ? 0 : kw;
     B->npos += npos;
     B->nneg += nneg;
-    B->flops += flops;
-    if (k >= ncand) B->state = 1;
+    B->flops += flops + uflops;
+    atomicAdd(s.flops + 1, flops);
+    if (FUSED)
+      B->state = 2;
+    else if (k >= ncand)
+      B->state = 1;
   }
 }
 
@@ -651,7 +692,11 @@ __global__ void big_after_update_kernel(DevState s, int nbig) {
   if (B.state == 2) return;
   if (B.kw > 0) {
     const double r = (double)(B.f - B.k);
-    B.flops += r * (r + 1.0) * B.kw;
+    const double fl = r * (r + 1.0) * B.kw;
+    B.flops += fl;
+    atomicAdd(s.flops + 2, fl);
+    // trailing lower triangle read and written, panel L and W rows read
+    atomicAdd(s.flops + 3, 8.0 * (r * (r + 1.0) + 2.0 * r * B.kw));
   }
   B.kw = 0;
   if (B.state == 1) B.state = 2;
@@ -681,7 +726,7 @@ __global__ void big_finalize_kernel(DevState s, int nbig, int cholesky) {
   atomicAdd(s.flops, B.flops);
 }
 
-template <int CL>
+template <int CL, bool FUSED>
 cudaError_t launch_panel(const DevState& s, const FactorParams& prm, int count, int NB,
                          size_t smem, cudaStream_t stream) {
   cudaLaunchConfig_t cfg = {};
@@ -696,7 +741,7 @@ cudaError_t launch_panel(const DevState& s, const FactorParams& prm, int count, 
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, big_panel_kernel<CL>, s, prm, NB);
+  return cudaLaunchKernelEx(&cfg, big_panel_kernel<CL, FUSED>, s, prm, NB, (int)smem);
 }
 
 constexpr size_t kPanelSmemMax = 224 * 1024;
@@ -705,54 +750,80 @@ constexpr size_t kPanelSmemMax = 224 * 1024;
 
 cudaError_t configure_big_kernels() {
   cudaError_t e;
-  e = cudaFuncSetAttribute(big_panel_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)kPanelSmemMax);
+  e = cudaFuncSetAttribute(big_panel_kernel<1, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(big_panel_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)kPanelSmemMax);
+  e = cudaFuncSetAttribute(big_panel_kernel<4, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(big_panel_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)kPanelSmemMax);
+  e = cudaFuncSetAttribute(big_panel_kernel<8, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(big_panel_kernel<16>,
+  e = cudaFuncSetAttribute(big_panel_kernel<16, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(big_panel_kernel<16, false>,
                               cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
 }
 
 cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
                              int maxkids, const FactorParams& prm, const double* vals,
-                             const double* diag, cudaStream_t stream) {
+                             const double* diag, cudaStream_t stream, Prof& prof) {
   const int nb = info.count;
   if (nb <= 0) return cudaSuccess;
   const int cols_per = 8;  // warps per CTA in the assembly kernels
   const int ychunks = std::min(256, (info.max_f + cols_per - 1) / cols_per);
+  prof.begin(stream);
   big_zero_kernel<<<dim3(nb, ychunks), 256, 0, stream>>>(s);
   big_scatter_kernel<<<dim3(nb, 16), 256, 0, stream>>>(p, s, vals, diag);
   if (diag) big_diag_kernel<<<nb, 256, 0, stream>>>(p, s, diag);
   for (int c = 0; c < maxkids; c++)
     big_extend_kernel<<<dim3(nb, ychunks), 256, 0, stream>>>(p, s, c);
+  prof.end(kPhBigAsm, stream, 2 + (diag ? 1 : 0) + maxkids);
 
-  // cluster size and panel width from the largest front of the level
-  int CL = info.max_f > 1536 ? 16 : (info.max_f > 512 ? 8 : 4);
+  // medium fronts: one CTA each, whole factorization in one launch
+  if (info.max_f_medium > 0) {
+    size_t msmem = (size_t)info.max_f_medium * (2 * (16 + 1) + 2) * sizeof(double);
+    if (msmem > kPanelSmemMax) msmem = kPanelSmemMax;
+    prof.begin(stream);
+    cudaError_t e = launch_panel<1, true>(s, prm, nb, 16, msmem, stream);
+    if (e != cudaSuccess) return e;
+    prof.end(kPhBigPanel, stream, 1);
+  }
+  if (info.count_large == 0) {
+    prof.begin(stream);
+    big_finalize_kernel<<<(nb + 255) / 256, 256, 0, stream>>>(s, nb, prm.cholesky);
+    prof.end(kPhBigAsm, stream, 1);
+    return cudaGetLastError();
+  }
+  // large fronts: a cluster per front and a panel per launch. Cluster size
+  // and panel width from the largest front: aim for <= 200 rows per CTA so
+  // that two CTAs fit on an SM.
+  int CL = info.max_f > 1600 ? 16 : 8;
   const int R = (info.max_f + CL - 1) / CL;
   int NB = kBigPanelMax;
-  while (NB > 4 && (size_t)R * (2 * NB + 2) * sizeof(double) > kPanelSmemMax) NB >>= 1;
-  const size_t smem = (size_t)R * (2 * NB + 2) * sizeof(double);
-  const int steps = (info.max_fs + (NB - 2)) / (NB - 1) + 1;
+  while (NB > 4 && (size_t)R * (2 * (NB + 1) + 2) * sizeof(double) > kPanelSmemMax) NB >>= 1;
+  const size_t smem = (size_t)R * (2 * (NB + 1) + 2) * sizeof(double);
+  const int steps = (info.max_fs_large + (NB - 2)) / (NB - 1) + 1;
   const int upd_grid = 148 * 4;
   for (int st = 0; st < steps; st++) {
     cudaError_t e;
+    prof.begin(stream);
     if (CL == 16)
-      e = launch_panel<16>(s, prm, nb, NB, smem, stream);
-    else if (CL == 8)
-      e = launch_panel<8>(s, prm, nb, NB, smem, stream);
+      e = launch_panel<16, false>(s, prm, nb, NB, smem, stream);
     else
-      e = launch_panel<4>(s, prm, nb, NB, smem, stream);
+      e = launch_panel<8, false>(s, prm, nb, NB, smem, stream);
     if (e != cudaSuccess) return e;
+    prof.end(kPhBigPanel, stream, 1);
+    prof.begin(stream);
     big_tiles_kernel<<<1, 1024, 0, stream>>>(s, nb);
     big_update_kernel<<<upd_grid, kUpdThreads, 0, stream>>>(s, nb);
     big_after_update_kernel<<<(nb + 255) / 256, 256, 0, stream>>>(s, nb);
+    prof.end(kPhBigUpd, stream, 3);
   }
+  prof.begin(stream);
   big_finalize_kernel<<<(nb + 255) / 256, 256, 0, stream>>>(s, nb, prm.cholesky);
+  prof.end(kPhBigAsm, stream, 1);
   return cudaGetLastError();
 }
 

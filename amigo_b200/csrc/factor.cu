@@ -30,6 +30,18 @@ __device__ __forceinline__ void keep_larger(double& bv, int& bi, double v, int i
   }
 }
 
+// Warp-wide (argmax, max) with the result in every lane.
+__device__ __forceinline__ void warp_argmax(double& bv, int& bi, double& cm) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    const double om = __shfl_xor_sync(0xffffffffu, cm, o);
+    keep_larger(bv, bi, ov, oi);
+    cm = fmax(cm, om);
+  }
+}
+
 struct Reduce {
   double v[kWarps];
   int i[kWarps];
@@ -176,6 +188,12 @@ __global__ void __launch_bounds__(kFactorThreads)
       const int slot = atomicAdd(s.big_meta, 1);
       atomicMax(s.big_meta + 1, f);
       atomicMax(s.big_meta + 2, fs);
+      if (f > kMediumMax) {
+        atomicAdd(s.big_meta + 3, 1);
+        atomicMax(s.big_meta + 4, fs);
+      } else {
+        atomicMax(s.big_meta + 5, f);
+      }
       BigFront b;
       b.node = node;
       b.f = f;
@@ -288,69 +306,79 @@ __global__ void __launch_bounds__(kFactorThreads)
     }
   }
 
-  // partial factorization of the fully summed candidates [0, ncand)
+  // partial factorization of the fully summed candidates [0, ncand).
+  // Right-looking, one barrier per accepted 1x1 pivot: the warp that updates
+  // the next column also produces its pivot statistics, and the scaling of
+  // a pivot column into L is deferred to the next update pass (it is a
+  // per-row operation, so it commutes with the row interchanges in between).
   const bool root = (nc == 0);
   const double alpha_bk = (1.0 + 4.1231056256176605) / 8.0;  // (1 + sqrt(17)) / 8
+  __shared__ double st_v, st_m;
+  __shared__ int st_i;
   int k = 0;
   int ncand = fs;
   int npos = 0, nneg = 0;
   double flops = 0.0;
-  // scratch for the unscaled pivot columns (2 x f), after the front
-  double* w0 = F + (size_t)ld * f;
-  double* w1 = w0 + f;
+  int pend = 0, pc = 0;
+  double pd0 = 0.0, pd1 = 0.0, pd2 = 0.0;
+  bool need_stats = true;
 
   while (k < ncand) {
+    if (!prm.cholesky && need_stats) {
+      if (warp == 0) {
+        double bv = -1.0, cm = 0.0;
+        int bi = INT_MAX;
+        const double* colk = F + (size_t)ld * k;
+        for (int i = k + 1 + lane; i < f; i += 32) {
+          const double a = fabs(colk[i]);
+          if (i < ncand)
+            keep_larger(bv, bi, a, i);
+          else
+            cm = fmax(cm, a);
+        }
+        warp_argmax(bv, bi, cm);
+        if (lane == 0) {
+          st_v = bv;
+          st_i = bi;
+          st_m = cm;
+        }
+      }
+      __syncthreads();
+    }
     int step;
     int kpiv = k;
     if (prm.cholesky) {
       step = kOne;
     } else {
-      double bv = -1.0, cmx = 0.0;
-      int bi = INT_MAX;
-      const double* colk = F + (size_t)ld * k;
-      for (int i = k + 1 + tid; i < f; i += blockDim.x) {
-        const double a = fabs(colk[i]);
-        if (i < ncand)
-          keep_larger(bv, bi, a, i);
-        else
-          cmx = fmax(cmx, a);
-      }
-      block_argmax(red, bv, bi, cmx);
-      const double wkk = colk[k];
+      const double wkk = F[k + (size_t)ld * k];
       const double abswkk = fabs(wkk);
       const bool has_cand = (k + 1 < ncand);
-      const double abswik = has_cand ? bv : 0.0;
-      // bi stays INT_MAX only if every candidate entry is NaN; keep imax a
+      const double abswik = has_cand ? st_v : 0.0;
+      // st_i stays INT_MAX only if every candidate entry is NaN; keep imax a
       // valid candidate index so the rest of the step stays in bounds
-      const int imax = has_cand ? (bi < ncand ? bi : k + 1) : k;
-      const double colmax = fmax(abswik, cmx);
+      const int imax = has_cand ? (st_i < ncand ? st_i : k + 1) : k;
+      const double colmax = fmax(abswik, st_m);
       if (root) {
-        if (fmax(abswkk, colmax) == 0.0) {
+        if (fmax(abswkk, colmax) == 0.0)
           step = kZero;
-        } else if (abswkk >= alpha_bk * colmax) {
+        else if (abswkk >= alpha_bk * colmax)
           step = kOne;
-        } else {
+        else
           step = kNeedRow;
-        }
       } else if (abswkk >= prm.pivot_tol && abswkk >= prm.ustab * colmax) {
         step = kOne;
-      } else if (has_cand) {
-        step = kNeedRow;
       } else {
-        step = kDelay;
+        step = has_cand ? kNeedRow : kDelay;
       }
       if (step == kNeedRow) {
-        // row/column imax outside the diagonal: F(imax, k:imax), F(imax+1:, imax)
+        // row/column imax off the diagonal: F(imax, k:imax), F(imax+1:, imax)
         double rv = -1.0, rmax = 0.0;
         int ri = INT_MAX;
         const int n1 = imax - k;
         const int n2 = f - imax - 1;
         for (int t = tid; t < n1 + n2; t += blockDim.x) {
-          double a;
-          if (t < n1)
-            a = fabs(F[imax + (size_t)ld * (k + t)]);
-          else
-            a = fabs(F[(imax + 1 + (t - n1)) + (size_t)ld * imax]);
+          const double a = (t < n1) ? fabs(F[imax + (size_t)ld * (k + t)])
+                                    : fabs(F[(imax + 1 + (t - n1)) + (size_t)ld * imax]);
           rmax = fmax(rmax, a);
         }
         block_argmax(red, rv, ri, rmax);
@@ -373,15 +401,12 @@ __global__ void __launch_bounds__(kFactorThreads)
           kpiv = imax;
         } else {
           const double det = fabs(wkk * wii - wik * wik);
-          if (det < prm.pivot_tol) {
-            step = kDelay;
-          } else {
+          step = kDelay;
+          if (det >= prm.pivot_tol) {
             const double delta = det / fmax(abswii + abswik, abswkk + abswik);
             if (delta >= prm.ustab * colmax && delta >= prm.ustab * rmax) {
               step = kTwo;
               kpiv = imax;
-            } else {
-              step = kDelay;
             }
           }
         }
@@ -392,6 +417,7 @@ __global__ void __launch_bounds__(kFactorThreads)
       if (k < ncand - 1) symm_swap(F, ld, f, k, ncand - 1, fv, orig);
       __syncthreads();
       ncand -= 1;
+      need_stats = true;
       continue;
     }
     const int nstep = (step == kTwo) ? 2 : 1;
@@ -401,22 +427,52 @@ __global__ void __launch_bounds__(kFactorThreads)
       __syncthreads();
     }
 
-    double* colk = F + (size_t)ld * k;
+    // deferred scaling of the previous pivot column(s)
+    if (pend == 1) {
+      double* c0 = F + (size_t)ld * pc;
+      for (int i = pc + 1 + tid; i < f; i += blockDim.x) c0[i] *= pd0;
+    } else if (pend == 2) {
+      double* c0 = F + (size_t)ld * pc;
+      double* c1 = c0 + ld;
+      for (int i = pc + 2 + tid; i < f; i += blockDim.x) {
+        const double a = c0[i];
+        const double b = c1[i];
+        c0[i] = a * pd0 + b * pd1;
+        c1[i] = a * pd1 + b * pd2;
+      }
+    }
+
+    const double* colk = F + (size_t)ld * k;
+    const int nxt = k + nstep;  // the next candidate column
+    const bool want_stats = !prm.cholesky && nxt < ncand;
     if (nstep == 1) {
       const double d = colk[k];
-      const bool zero = (step == kZero) || (d == 0.0 && root);
-      const double dinv = zero ? 0.0 : 1.0 / d;
-      for (int i = k + 1 + tid; i < f; i += blockDim.x) {
-        const double w = colk[i];
-        w0[i] = w;
-        colk[i] = w * dinv;
-      }
-      __syncthreads();
-      if (!zero) {
-        for (int j = k + 1 + warp; j < f; j += kWarps) {
-          const double wj = w0[j];
-          double* colj = F + (size_t)ld * j;
-          for (int i = j + lane; i < f; i += 32) colj[i] -= colk[i] * wj;
+      const double dinv = (step == kZero || (root && d == 0.0)) ? 0.0 : 1.0 / d;
+      for (int j = k + 1 + warp; j < f; j += kWarps) {
+        const double lj = colk[j] * dinv;
+        double* colj = F + (size_t)ld * j;
+        if (j == nxt && want_stats) {
+          double bv = -1.0, cm = 0.0;
+          int bi = INT_MAX;
+          for (int i = j + lane; i < f; i += 32) {
+            const double v = colj[i] - colk[i] * lj;
+            colj[i] = v;
+            if (i > j) {
+              const double a = fabs(v);
+              if (i < ncand)
+                keep_larger(bv, bi, a, i);
+              else
+                cm = fmax(cm, a);
+            }
+          }
+          warp_argmax(bv, bi, cm);
+          if (lane == 0) {
+            st_v = bv;
+            st_i = bi;
+            st_m = cm;
+          }
+        } else {
+          for (int i = j + lane; i < f; i += 32) colj[i] -= colk[i] * lj;
         }
       }
       if (tid == 0) {
@@ -427,25 +483,50 @@ __global__ void __launch_bounds__(kFactorThreads)
         const double r = (double)(f - k - 1);
         flops += r * (r + 1.0) + r;
       }
+      pend = 1;
+      pc = k;
+      pd0 = dinv;
     } else {
-      double* colk1 = colk + ld;
+      const double* colk1 = colk + ld;
       const double d11 = colk[k];
       const double d21 = colk[k + 1];
       const double d22 = colk1[k + 1];
-      const double detinv = 1.0 / (d11 * d22 - d21 * d21);
+      const double det = d11 * d22 - d21 * d21;
+      const double detinv = 1.0 / det;
       const double i00 = d22 * detinv, i01 = -d21 * detinv, i11 = d11 * detinv;
-      for (int i = k + 2 + tid; i < f; i += blockDim.x) {
-        const double a = colk[i];
-        const double b = colk1[i];
-        w0[i] = a;
-        w1[i] = b;
-        colk[i] = a * i00 + b * i01;
-        colk1[i] = a * i01 + b * i11;
+      for (int j = k + 2 + warp; j < f; j += kWarps) {
+        const double a = colk[j];
+        const double b = colk1[j];
+        const double l0 = a * i00 + b * i01;
+        const double l1 = a * i01 + b * i11;
+        double* colj = F + (size_t)ld * j;
+        if (j == nxt && want_stats) {
+          double bv = -1.0, cm = 0.0;
+          int bi = INT_MAX;
+          for (int i = j + lane; i < f; i += 32) {
+            const double v = colj[i] - (colk[i] * l0 + colk1[i] * l1);
+            colj[i] = v;
+            if (i > j) {
+              const double aa = fabs(v);
+              if (i < ncand)
+                keep_larger(bv, bi, aa, i);
+              else
+                cm = fmax(cm, aa);
+            }
+          }
+          warp_argmax(bv, bi, cm);
+          if (lane == 0) {
+            st_v = bv;
+            st_i = bi;
+            st_m = cm;
+          }
+        } else {
+          for (int i = j + lane; i < f; i += 32) colj[i] -= colk[i] * l0 + colk1[i] * l1;
+        }
       }
       if (tid == 0) {
         fv[k] = -(fv[k] + 1);
         fv[k + 1] = -(fv[k + 1] + 1);
-        const double det = d11 * d22 - d21 * d21;
         if (det >= 0.0) {
           if (d11 >= 0.0)
             npos += 2;
@@ -458,17 +539,32 @@ __global__ void __launch_bounds__(kFactorThreads)
         const double r = (double)(f - k - 2);
         flops += 2.0 * r * (r + 1.0) + 6.0 * r;
       }
-      __syncthreads();
-      for (int j = k + 2 + warp; j < f; j += kWarps) {
-        const double a = w0[j];
-        const double b = w1[j];
-        double* colj = F + (size_t)ld * j;
-        for (int i = j + lane; i < f; i += 32) colj[i] -= colk[i] * a + colk1[i] * b;
-      }
+      pend = 2;
+      pc = k;
+      pd0 = i00;
+      pd1 = i01;
+      pd2 = i11;
     }
     __syncthreads();
+    // the warp owning column nxt covered every row below it only if nxt < f
+    need_stats = !(want_stats);
     k += nstep;
   }
+  // last deferred scaling
+  if (pend == 1) {
+    double* c0 = F + (size_t)ld * pc;
+    for (int i = pc + 1 + tid; i < f; i += blockDim.x) c0[i] *= pd0;
+  } else if (pend == 2) {
+    double* c0 = F + (size_t)ld * pc;
+    double* c1 = c0 + ld;
+    for (int i = pc + 2 + tid; i < f; i += blockDim.x) {
+      const double a = c0[i];
+      const double b = c1[i];
+      c0[i] = a * pd0 + b * pd1;
+      c1[i] = a * pd1 + b * pd2;
+    }
+  }
+  __syncthreads();
 
   const int npiv = k;
   const int m = f - npiv;

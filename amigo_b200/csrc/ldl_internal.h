@@ -4,8 +4,77 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <utility>
+#include <vector>
 
 namespace b200ldl {
+
+// Kernel classes timed by the optional profiler.
+enum ProfPhase : int {
+  kPhFront = 0,     // per-level front kernels (assembly + factor in shared memory)
+  kPhBigAsm = 1,    // big-front assembly (zero, scatter, extend-add)
+  kPhBigPanel = 2,  // cluster panel factorization
+  kPhBigUpd = 3,    // tiled trailing update
+  kPhFwd = 4,       // forward solve
+  kPhBwd = 5,       // backward solve
+  kPhN = 6
+};
+
+// CUDA-event timing of kernel classes on the launching stream, plus a count
+// of kernels launched. Events are recorded only while `on`.
+struct Prof {
+  bool on = false;
+  std::vector<cudaEvent_t> pool;
+  size_t used = 0;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+  double ms[kPhN] = {};
+  long long launches[kPhN] = {};
+  long long total_launches = 0;
+  cudaEvent_t cur = nullptr;
+
+  cudaEvent_t next() {
+    if (used == pool.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      pool.push_back(e);
+    }
+    return pool[used++];
+  }
+  void begin(cudaStream_t st) {
+    if (!on) return;
+    cur = next();
+    cudaEventRecord(cur, st);
+  }
+  void end(int phase, cudaStream_t st, int nlaunch) {
+    total_launches += nlaunch;
+    launches[phase] += nlaunch;
+    if (!on) return;
+    cudaEvent_t e = next();
+    cudaEventRecord(e, st);
+    marks.push_back({phase, {cur, e}});
+  }
+  // after the stream has been synchronized
+  void collect() {
+    for (auto& m : marks) {
+      float t = 0.f;
+      if (cudaEventElapsedTime(&t, m.second.first, m.second.second) == cudaSuccess)
+        ms[m.first] += t;
+    }
+    marks.clear();
+    used = 0;
+  }
+  void reset() {
+    for (int i = 0; i < kPhN; i++) {
+      ms[i] = 0.0;
+      launches[i] = 0;
+    }
+    marks.clear();
+    used = 0;
+  }
+  ~Prof() {
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+};
 
 // Immutable per-pattern data uploaded once after the symbolic phase. All
 // arrays are indexed by supernode id (the reference's node numbering) unless
@@ -62,7 +131,8 @@ struct DevState {
   int64_t* u_off;   // [nn] into the solve's update-vector pool (units of rows)
   int* err;         // [4]: [0] overflow flag, [1] node of first error
   int* inertia;     // [2] pos, neg
-  double* flops;    // [1] executed factor flops (accumulated)
+  double* flops;    // [4] executed flops: [0] all fronts, [1] big panels,
+                    // [2] big trailing updates, [3] trailing-update bytes moved
   BigFront* big;    // [nn] big fronts of the current level
   int* big_meta;    // [4]: count, max f, max fs, unused
   long long* tile_ptr;  // [nn+1] update tiles per big front (prefix)
@@ -89,23 +159,29 @@ size_t factor_smem_bytes();
 // number of children among the level's supernodes.
 struct BigLevelInfo {
   int count, max_f, max_fs;
+  int count_large, max_fs_large, max_f_medium;
 };
+
+// Fronts above kSmemFrontMax and up to kMediumMax are factored by one CTA in
+// a single launch; larger ones by a thread-block cluster per panel.
+constexpr int kMediumMax = 768;
 cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
-                      int maxkids, const FactorParams& prm, const double* vals,
-                      const double* diag, cudaStream_t stream);
+                             int maxkids, const FactorParams& prm, const double* vals,
+                             const double* diag, cudaStream_t stream, Prof& prof);
 cudaError_t configure_big_kernels();
 
 constexpr int kSolveThreads = 256;
-// Front vectors of the solve live in shared memory up to this front size.
-constexpr int kSolveSmemFront = 12288;
+// Right-hand sides per solve launch for a level whose largest front is fmax
+// (0 if even one does not fit in shared memory).
+int solve_rhs_chunk(int fmax, int nrhs);
 
-void launch_forward_level(const DevPlan& p, const DevState& s,
+int launch_forward_level(const DevPlan& p, const DevState& s,
+                         const int* level_nodes, int count, double* x,
+                         int ldx, int nrhs, double* upool, int fmax,
+                         cudaStream_t stream);
+int launch_backward_level(const DevPlan& p, const DevState& s,
                           const int* level_nodes, int count, double* x,
-                          int ldx, int nrhs, double* upool, int fmax,
-                          cudaStream_t stream);
-void launch_backward_level(const DevPlan& p, const DevState& s,
-                           const int* level_nodes, int count, double* x,
-                           int ldx, int nrhs, int fmax, cudaStream_t stream);
+                          int ldx, int nrhs, int fmax, cudaStream_t stream);
 cudaError_t configure_solve_kernels();
 
 }  // namespace b200ldl

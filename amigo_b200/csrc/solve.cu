@@ -16,7 +16,9 @@
 // 1825-1926: solve_pivot_lower, L21 product, scatter_subtract,
 // solve_pivot_diagonal, and the transposed sweep), reorganised so that the
 // descendants' contributions travel as update vectors instead of
-// scatter-subtracts into the shared solution vector.
+// scatter-subtracts into the shared solution vector, and blocked: one warp
+// solves each diagonal block of up to 33 pivots while the whole CTA applies
+// the block to the rows below, with all right-hand sides of a chunk at once.
 #include "ldl_internal.h"
 
 namespace b200ldl {
@@ -24,28 +26,155 @@ namespace b200ldl {
 namespace {
 
 constexpr int kSWarps = kSolveThreads / 32;
+constexpr int kBlk = 32;
 
-__device__ __forceinline__ double block_sum(double v, double* red) {
-  const int lane = threadIdx.x & 31;
-  const int w = threadIdx.x >> 5;
+constexpr int kMaxRhs = 8;  // right-hand sides per launch
+
+// v[r][j] -= sum_{i in [i0, i1)} L(i, j) v[r][i] for r < nr, by one warp
+__device__ __forceinline__ void gemv_t_col(const double* L, int ldl, int j, int i0, int i1,
+                                           double* v, int f, int nr, int lane) {
+  const double* lj = L + (size_t)ldl * j;
+  double acc[kMaxRhs];
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  if (lane == 0) red[w] = v;
-  __syncthreads();
-  double t = 0.0;
+  for (int r = 0; r < kMaxRhs; r++) acc[r] = 0.0;
+  for (int i = i0 + lane; i < i1; i += 32) {
+    const double l = lj[i];
 #pragma unroll
-  for (int q = 0; q < kSWarps; q++) t += red[q];
-  __syncthreads();
-  return t;
+    for (int r = 0; r < kMaxRhs; r++)
+      if (r < nr) acc[r] += l * v[(size_t)r * f + i];
+  }
+#pragma unroll
+  for (int r = 0; r < kMaxRhs; r++) {
+    if (r < nr) {
+      double a = acc[r];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+      if (lane == 0) v[(size_t)r * f + j] -= a;
+    }
+  }
+}
+
+// end of the pivot block starting at jb: at most 32 pivots, and 2x2 pairs
+// never straddle two blocks
+__device__ __forceinline__ int block_end(const int* fv, int jb, int npiv) {
+  int j = jb;
+  while (j < npiv) {
+    const int st = (fv[j] >= 0) ? 1 : 2;
+    if (j + st - jb > kBlk) break;
+    j += st;
+  }
+  return j;
+}
+
+// Bit t set if position jb + t is the second row of a 2x2 pivot. Blocks
+// start on a pair boundary, so inside a run of negative (2x2-marked) entries
+// the odd offsets are the second rows.
+__device__ __forceinline__ unsigned second_rows(const int* fv, int jb, int je, int lane) {
+  const bool neg = (jb + lane < je) && fv[jb + lane] < 0;
+  const unsigned negm = __ballot_sync(0xffffffffu, neg);
+  const unsigned below = lane == 0 ? 0u : (~negm) & ((1u << lane) - 1u);
+  const int start = below ? (32 - __clz(below)) : 0;
+  return __ballot_sync(0xffffffffu, neg && ((lane - start) & 1));
+}
+
+// Warp 0: forward substitution with the unit-lower diagonal block (rows and
+// columns [jb, je), at most 32) held in registers (lane t owns row jb + t),
+// then D^{-1} to the solution at the block's pivot variables.
+__device__ __forceinline__ void fwd_block(const double* L, int ldl, const int* fv, int jb,
+                                          int je, double* v, int f, int nr, double* x,
+                                          int ldx, int r0, int lane) {
+  const int nb = je - jb;
+  const unsigned sec = second_rows(fv, jb, je, lane);
+  const bool mine = lane < nb;
+  double Lrow[kBlk];
+#pragma unroll
+  for (int j = 0; j < kBlk; j++)
+    Lrow[j] = (mine && j < nb) ? L[(jb + lane) + (size_t)ldl * (jb + j)] : 0.0;
+  double vr[kMaxRhs];
+#pragma unroll
+  for (int r = 0; r < kMaxRhs; r++) vr[r] = (mine && r < nr) ? v[(size_t)r * f + jb + lane] : 0.0;
+#pragma unroll
+  for (int j = 0; j < kBlk; j++) {
+    if (j < nb) {
+      const bool first = j + 1 < nb && ((sec >> (j + 1)) & 1u);
+      const bool upd = lane > j && !(first && lane == j + 1);
+#pragma unroll
+      for (int r = 0; r < kMaxRhs; r++) {
+        const double vj = __shfl_sync(0xffffffffu, vr[r], j);
+        if (upd && r < nr) vr[r] = fma(-Lrow[j], vj, vr[r]);
+      }
+    }
+  }
+  // D^{-1}: 1x1 pivots divide; 2x2 pairs exchange values with the partner
+  const bool is_sec = (sec >> lane) & 1u;
+  const bool is_first = lane + 1 < 32 && ((sec >> (lane + 1)) & 1u) && lane + 1 < nb;
+  const double dd = mine ? L[(jb + lane) + (size_t)ldl * (jb + lane)] : 1.0;
+  const double dsub = (mine && is_sec) ? L[(jb + lane) + (size_t)ldl * (jb + lane - 1)] : 0.0;
+  const double dd_up = __shfl_down_sync(0xffffffffu, dd, 1);
+  const double dsub_up = __shfl_down_sync(0xffffffffu, dsub, 1);
+  const double dd_dn = __shfl_up_sync(0xffffffffu, dd, 1);
+  const int var = mine ? fv[jb + lane] : 0;
+  const int vi = var >= 0 ? var : -var - 1;
+#pragma unroll
+  for (int r = 0; r < kMaxRhs; r++) {
+    const double up = __shfl_down_sync(0xffffffffu, vr[r], 1);
+    const double dn = __shfl_up_sync(0xffffffffu, vr[r], 1);
+    if (mine && r < nr) {
+      double y;
+      if (is_first) {
+        const double d11 = dd, d21 = dsub_up, d22 = dd_up;
+        y = (d22 * vr[r] - d21 * up) / (d11 * d22 - d21 * d21);
+      } else if (is_sec) {
+        const double d11 = dd_dn, d21 = dsub, d22 = dd;
+        y = (d11 * vr[r] - d21 * dn) / (d11 * d22 - d21 * d21);
+      } else {
+        y = vr[r] / dd;
+      }
+      x[(size_t)ldx * (r0 + r) + vi] = y;
+      v[(size_t)r * f + jb + lane] = vr[r];
+    }
+  }
+}
+
+// Warp 0: back substitution with the transposed block L11^T (lane t owns
+// row jb + t and keeps column jb + t of the block in registers).
+__device__ __forceinline__ void bwd_block(const double* L, int ldl, const int* fv, int jb,
+                                          int je, double* v, int f, int nr, int lane) {
+  const int nb = je - jb;
+  const unsigned sec = second_rows(fv, jb, je, lane);
+  const bool mine = lane < nb;
+  double Lcol[kBlk];
+  const double* col = L + (size_t)ldl * (jb + lane) + jb;
+#pragma unroll
+  for (int q = 0; q < kBlk; q++) Lcol[q] = (mine && q < nb) ? col[q] : 0.0;
+  double vr[kMaxRhs];
+#pragma unroll
+  for (int r = 0; r < kMaxRhs; r++) vr[r] = (mine && r < nr) ? v[(size_t)r * f + jb + lane] : 0.0;
+#pragma unroll
+  for (int jj = kBlk - 1; jj >= 0; jj--) {
+    if (jj < nb) {
+      const bool upd = lane < jj && !(((sec >> jj) & 1u) && lane == jj - 1);
+#pragma unroll
+      for (int r = 0; r < kMaxRhs; r++) {
+        const double vj = __shfl_sync(0xffffffffu, vr[r], jj);
+        if (upd && r < nr) vr[r] = fma(-Lcol[jj], vj, vr[r]);
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kMaxRhs; r++)
+    if (mine && r < nr) v[(size_t)r * f + jb + lane] = vr[r];
 }
 
 __global__ void __launch_bounds__(kSolveThreads)
     forward_level_kernel(DevPlan p, DevState s, const int* __restrict__ nodes,
-                         double* __restrict__ x, int ldx, int nrhs,
+                         double* __restrict__ x, int ldx, int nrhs, int r0, int nr,
                          double* __restrict__ upool) {
   extern __shared__ __align__(16) double sm[];
   const int node = nodes[blockIdx.x];
   const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
   const int f = s.f[node];
   const int fs = s.fs[node];
   const int npiv = s.npiv[node];
@@ -58,73 +187,76 @@ __global__ void __launch_bounds__(kSolveThreads)
   const int ldl = s.L_ld[node];
   const int kb = p.kid_ptr[node];
   const int ke = p.kid_ptr[node + 1];
-  double* w = sm;      // pre-pivot order
-  double* v = sm + f;  // post-pivot order
+  double* v = sm;                          // [nr][f], post-pivot order
+  int* post_of = (int*)(sm + (size_t)nr * f);  // [f]
 
-  for (int r = 0; r < nrhs; r++) {
-    double* xr = x + (size_t)ldx * r;
-    const int v0 = p.var_ptr[node];
-    for (int t = tid; t < f; t += blockDim.x)
-      w[t] = (t < ns) ? xr[p.node_to_var[v0 + t]] : 0.0;
-    __syncthreads();
-    int off = ns;
-    for (int c = kb; c < ke; c++) {
-      const int ch = p.kids[c];
-      const int nd = s.ndel[ch];
-      const int mc = s.f[ch] - s.npiv[ch];
-      const double* uc = upool + s.u_off[ch] * nrhs + (size_t)r * mc;
-      const int* cm = p.cmap + p.cptr[ch];
-      for (int t = tid; t < mc; t += blockDim.x) {
-        int q;
-        if (t < nd) {
-          q = off + t;
-        } else {
-          q = cm[t - nd];
-          if (q >= ns) q += nd_in;
-        }
-        w[q] += uc[t];
-      }
-      __syncthreads();
-      off += nd;
-    }
-    for (int t = tid; t < f; t += blockDim.x) v[t] = (t < fs) ? w[orig[t]] : w[t];
-    __syncthreads();
-
-    for (int j = 0; j < npiv;) {
-      if (fv[j] >= 0) {
-        const double vj = v[j];
-        const double* lj = L + (size_t)ldl * j;
-        for (int i = j + 1 + tid; i < f; i += blockDim.x) v[i] -= lj[i] * vj;
-        if (tid == 0) xr[fv[j]] = vj / lj[j];
-        __syncthreads();
-        j += 1;
+  for (int q = tid; q < f; q += blockDim.x) post_of[q < fs ? orig[q] : q] = q;
+  for (int q = tid; q < nr * f; q += blockDim.x) v[q] = 0.0;
+  __syncthreads();
+  const int v0 = p.var_ptr[node];
+  for (int q = tid; q < nr * ns; q += blockDim.x) {
+    const int r = q / ns;
+    const int t = q - r * ns;
+    v[(size_t)r * f + post_of[t]] = x[(size_t)ldx * (r0 + r) + p.node_to_var[v0 + t]];
+  }
+  __syncthreads();
+  int off = ns;
+  for (int c = kb; c < ke; c++) {
+    const int ch = p.kids[c];
+    const int nd = s.ndel[ch];
+    const int mc = s.f[ch] - s.npiv[ch];
+    const double* uc = upool + s.u_off[ch] * nrhs + (size_t)r0 * mc;
+    const int* cm = p.cmap + p.cptr[ch];
+    for (int t = tid; t < mc; t += blockDim.x) {
+      int q;
+      if (t < nd) {
+        q = off + t;
       } else {
-        const double a = v[j];
-        const double b = v[j + 1];
-        const double* l0 = L + (size_t)ldl * j;
-        const double* l1 = l0 + ldl;
-        for (int i = j + 2 + tid; i < f; i += blockDim.x) v[i] -= l0[i] * a + l1[i] * b;
-        if (tid == 0) {
-          const double d11 = l0[j], d21 = l0[j + 1], d22 = l1[j + 1];
-          const double inv = 1.0 / (d11 * d22 - d21 * d21);
-          xr[-fv[j] - 1] = inv * (d22 * a - d21 * b);
-          xr[-fv[j + 1] - 1] = inv * (d11 * b - d21 * a);
-        }
-        __syncthreads();
-        j += 2;
+        q = cm[t - nd];
+        if (q >= ns) q += nd_in;
       }
+      q = post_of[q];
+      for (int r = 0; r < nr; r++) v[(size_t)r * f + q] += uc[(size_t)r * mc + t];
     }
-    double* uo = upool + s.u_off[node] * nrhs + (size_t)r * m;
-    for (int t = tid; t < m; t += blockDim.x) uo[t] = v[npiv + t];
     __syncthreads();
+    off += nd;
+  }
+
+  // blocked unit-lower solve: warp 0 solves the diagonal block in registers
+  // and writes D^{-1} t to the solution; then the CTA updates the rows below
+  for (int jb = 0; jb < npiv;) {
+    const int je = block_end(fv, jb, npiv);
+    if (warp == 0) fwd_block(L, ldl, fv, jb, je, v, f, nr, x, ldx, r0, lane);
+    __syncthreads();
+    for (int i = je + tid; i < f; i += blockDim.x) {
+      double acc[kMaxRhs];
+#pragma unroll
+      for (int r = 0; r < kMaxRhs; r++) acc[r] = 0.0;
+      for (int j = jb; j < je; j++) {
+        const double l = L[i + (size_t)ldl * j];
+#pragma unroll
+        for (int r = 0; r < kMaxRhs; r++)
+          if (r < nr) acc[r] = fma(l, v[(size_t)r * f + j], acc[r]);
+      }
+#pragma unroll
+      for (int r = 0; r < kMaxRhs; r++)
+        if (r < nr) v[(size_t)r * f + i] -= acc[r];
+    }
+    __syncthreads();
+    jb = je;
+  }
+  double* uo = upool + s.u_off[node] * nrhs + (size_t)r0 * m;
+  for (int q = tid; q < nr * m; q += blockDim.x) {
+    const int r = q / m;
+    const int t = q - r * m;
+    uo[(size_t)r * m + t] = v[(size_t)r * f + npiv + t];
   }
 }
 
 __global__ void __launch_bounds__(kSolveThreads)
     backward_level_kernel(DevPlan p, DevState s, const int* __restrict__ nodes,
-                          double* __restrict__ x, int ldx, int nrhs) {
+                          double* __restrict__ x, int ldx, int r0, int nr) {
   extern __shared__ __align__(16) double sm[];
-  __shared__ double red[kSWarps];
   const int node = nodes[blockIdx.x];
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -134,88 +266,103 @@ __global__ void __launch_bounds__(kSolveThreads)
   const int* fv = s.ivars + s.fv_off[node];
   const double* L = s.dpool + s.L_off[node];
   const int ldl = s.L_ld[node];
-  double* v = sm;
+  double* v = sm;                           // [nr][f]
+  int* bst = (int*)(sm + (size_t)nr * f);   // block starts
 
-  for (int r = 0; r < nrhs; r++) {
-    double* xr = x + (size_t)ldx * r;
-    for (int t = tid; t < f; t += blockDim.x) {
-      const int var = fv[t];
-      v[t] = xr[var >= 0 ? var : -var - 1];
+  for (int q = tid; q < nr * f; q += blockDim.x) {
+    const int r = q / f;
+    const int t = q - r * f;
+    const int var = fv[t];
+    v[q] = x[(size_t)ldx * (r0 + r) + (var >= 0 ? var : -var - 1)];
+  }
+  __shared__ int nblk;
+  if (tid == 0) {
+    int nb = 0;
+    for (int jb = 0; jb < npiv;) {
+      bst[nb++] = jb;
+      jb = block_end(fv, jb, npiv);
     }
+    bst[nb] = npiv;
+    nblk = nb;
+  }
+  __syncthreads();
+  // t1 -= L21^T x2, one warp per pivot column, all RHS per L read
+  if (npiv < f) {
+    for (int j = warp; j < npiv; j += kSWarps) gemv_t_col(L, ldl, j, npiv, f, v, f, nr, lane);
     __syncthreads();
-    // t1 -= L21^T x2, one warp per pivot column
-    for (int j = warp; j < npiv; j += kSWarps) {
-      const double* lj = L + (size_t)ldl * j;
-      double acc = 0.0;
-      for (int i = npiv + lane; i < f; i += 32) acc += lj[i] * v[i];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-      if (lane == 0) v[j] -= acc;
+  }
+  // L11^T back substitution, block by block from the last
+  for (int b = nblk - 1; b >= 0; b--) {
+    const int jb = bst[b];
+    const int je = bst[b + 1];
+    if (je < npiv) {
+      for (int j = jb + warp; j < je; j += kSWarps) gemv_t_col(L, ldl, j, je, npiv, v, f, nr, lane);
+      __syncthreads();
     }
+    if (warp == 0) bwd_block(L, ldl, fv, jb, je, v, f, nr, lane);
     __syncthreads();
-    // L11^T back substitution
-    for (int j = npiv - 1; j >= 0;) {
-      if (fv[j] >= 0) {
-        const double* lj = L + (size_t)ldl * j;
-        double acc = 0.0;
-        for (int i = j + 1 + tid; i < npiv; i += blockDim.x) acc += lj[i] * v[i];
-        acc = block_sum(acc, red);
-        if (tid == 0) v[j] -= acc;
-        __syncthreads();
-        j -= 1;
-      } else {
-        const double* l0 = L + (size_t)ldl * (j - 1);
-        const double* l1 = l0 + ldl;
-        double a0 = 0.0, a1 = 0.0;
-        for (int i = j + 1 + tid; i < npiv; i += blockDim.x) {
-          a0 += l0[i] * v[i];
-          a1 += l1[i] * v[i];
-        }
-        a0 = block_sum(a0, red);
-        a1 = block_sum(a1, red);
-        if (tid == 0) {
-          v[j - 1] -= a0;
-          v[j] -= a1;
-        }
-        __syncthreads();
-        j -= 2;
-      }
-    }
-    for (int t = tid; t < npiv; t += blockDim.x) {
-      const int var = fv[t];
-      xr[var >= 0 ? var : -var - 1] = v[t];
-    }
-    __syncthreads();
+  }
+  for (int q = tid; q < nr * npiv; q += blockDim.x) {
+    const int r = q / npiv;
+    const int t = q - r * npiv;
+    const int var = fv[t];
+    x[(size_t)ldx * (r0 + r) + (var >= 0 ? var : -var - 1)] = v[(size_t)r * f + t];
   }
 }
 
 }  // namespace
 
+constexpr size_t kSolveSmemMax = 224 * 1024;
+
 cudaError_t configure_solve_kernels() {
-  const int bytes = 2 * kSolveSmemFront * (int)sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(forward_level_kernel,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kSolveSmemMax);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(backward_level_kernel,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSolveSmemMax);
 }
 
-void launch_forward_level(const DevPlan& p, const DevState& s, const int* level_nodes,
-                          int count, double* x, int ldx, int nrhs, double* upool,
-                          int fmax, cudaStream_t stream) {
-  if (count <= 0) return;
-  const size_t smem = 2 * (size_t)fmax * sizeof(double);
-  forward_level_kernel<<<count, kSolveThreads, smem, stream>>>(p, s, level_nodes, x, ldx,
-                                                               nrhs, upool);
+// right-hand sides per launch so that [nr][fmax] doubles + fmax ints fit
+int solve_rhs_chunk(int fmax, int nrhs) {
+  const size_t per = (size_t)fmax * sizeof(double);
+  const size_t fixed = (size_t)fmax * sizeof(int) + 64;
+  if (fixed + per > kSolveSmemMax) return 0;
+  int c = (int)((kSolveSmemMax - fixed) / per);
+  if (c > kMaxRhs) c = kMaxRhs;
+  return c < nrhs ? c : nrhs;
 }
 
-void launch_backward_level(const DevPlan& p, const DevState& s, const int* level_nodes,
-                           int count, double* x, int ldx, int nrhs, int fmax,
-                           cudaStream_t stream) {
-  if (count <= 0) return;
-  const size_t smem = (size_t)fmax * sizeof(double);
-  backward_level_kernel<<<count, kSolveThreads, smem, stream>>>(p, s, level_nodes, x, ldx,
-                                                                nrhs);
+int launch_forward_level(const DevPlan& p, const DevState& s, const int* level_nodes,
+                         int count, double* x, int ldx, int nrhs, double* upool,
+                         int fmax, cudaStream_t stream) {
+  if (count <= 0) return 0;
+  const int c = solve_rhs_chunk(fmax, nrhs);
+  int n = 0;
+  for (int r0 = 0; r0 < nrhs; r0 += c) {
+    const int nr = (nrhs - r0 < c) ? nrhs - r0 : c;
+    const size_t smem = (size_t)nr * fmax * sizeof(double) + (size_t)fmax * sizeof(int);
+    forward_level_kernel<<<count, kSolveThreads, smem, stream>>>(p, s, level_nodes, x, ldx,
+                                                                 nrhs, r0, nr, upool);
+    n++;
+  }
+  return n;
+}
+
+int launch_backward_level(const DevPlan& p, const DevState& s, const int* level_nodes,
+                          int count, double* x, int ldx, int nrhs, int fmax,
+                          cudaStream_t stream) {
+  if (count <= 0) return 0;
+  const int c = solve_rhs_chunk(fmax, nrhs);
+  int n = 0;
+  for (int r0 = 0; r0 < nrhs; r0 += c) {
+    const int nr = (nrhs - r0 < c) ? nrhs - r0 : c;
+    const size_t smem = (size_t)nr * fmax * sizeof(double) + (size_t)fmax * sizeof(int);
+    backward_level_kernel<<<count, kSolveThreads, smem, stream>>>(p, s, level_nodes, x, ldx,
+                                                                  r0, nr);
+    n++;
+  }
+  return n;
 }
 
 }  // namespace b200ldl

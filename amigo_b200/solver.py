@@ -1,0 +1,108 @@
+"""The Amigo linear-solver plugin backed by the B200 factorization.
+
+``LinearSolver`` restates the reference's abstract base
+(amigo/algorithm/solvers/linear_solver.py:5-35) so that this package does not
+need Amigo importable. ``B200LdlSolver`` has AmigoSolver's constructor and
+methods (amigo/algorithm/solvers/amigo_solver.py:11-64), so
+``options["solver"] = B200LdlSolver(options, state)`` drops it into
+``make_solver`` (amigo/algorithm/solvers/__init__.py:16-19) unchanged. It
+works with Amigo's own CSRMat/Vector objects (host views through
+``get_nonzero_structure``/``get_data``/``[:]``) and with this package's
+CSRMat/Vector holding numpy arrays or torch CUDA tensors.
+"""
+
+from __future__ import annotations
+
+from abc import ABC, abstractmethod
+
+import numpy as np
+
+from .sparse_ldl import OrderingType, SolverType, SparseLDL, _is_torch, _values_of
+
+__all__ = ["LinearSolver", "B200LdlSolver"]
+
+
+class LinearSolver(ABC):
+    @abstractmethod
+    def factor(self, hess, diag):
+        return
+
+    @abstractmethod
+    def solve(self, b, x):
+        return
+
+    def inertia_enabled(self):
+        return False
+
+    def get_inertia(self):
+        return None
+
+    def set_pivot_tolerance(self, pivtol):
+        pass
+
+    @staticmethod
+    def find_diag_indices(rowp, cols, nrows):
+        """CSR data index of each diagonal entry (the reference helper of the
+        same name, linear_solver.py:24-35)."""
+        diag_idx = np.empty(nrows, dtype=np.intp)
+        for i in range(nrows):
+            start, end = rowp[i], rowp[i + 1]
+            pos = np.searchsorted(cols[start:end], i)
+            if pos < end - start and cols[start + pos] == i:
+                diag_idx[i] = start + pos
+            else:
+                diag_idx[i] = start
+        return diag_idx
+
+
+class B200LdlSolver(LinearSolver):
+    """AmigoSolver's contract on the GPU: symbolic analysis once for the
+    Hessian's pattern (AMD, ustab 0.01, pivot_tol 1e-14), numeric
+    factorization and inertia on every ``factor``, solve on the stored
+    factor."""
+
+    def __init__(self, options=None, state=None, hessian=None, ustab: float = 0.01,
+                 pivot_tol: float = 1e-14, order=OrderingType.DEFAULT):
+        self.options = options
+        self.hessian = hessian if hessian is not None else state.hessian
+        self.ldl = SparseLDL(self.hessian, SolverType.LDL, ustab=ustab, pivot_tol=pivot_tol,
+                             order=order)
+
+    def factor(self, hessian, diagonal):
+        if hessian is not self.hessian and hessian != self.hessian:
+            raise ValueError("Hessian instance must be the same")
+        # Amigo objects may keep the current values on the device; bring the
+        # host view up to date exactly as AmigoSolver does
+        if hasattr(diagonal, "copy_device_to_host"):
+            diagonal.copy_device_to_host()
+        if hasattr(self.hessian, "copy_data_device_to_host"):
+            self.hessian.copy_data_device_to_host()
+        flag = self.ldl.factor(diagonal)
+        if flag != 0:
+            raise RuntimeError(f"B200LdlSolver factorization failed with flag = {flag}")
+        return flag
+
+    def solve(self, b, x):
+        bv = _values_of(b)
+        if _is_torch(bv) and bv.is_cuda:
+            xv = _values_of(x)
+            xv.copy_(bv)
+            self.ldl.solve(xv)
+            return
+        rhs = np.array(bv[:] if not isinstance(bv, np.ndarray) else bv, dtype=np.float64)
+        self.ldl.solve(rhs)
+        if hasattr(x, "copy_host_to_device") and hasattr(x, "__setitem__"):
+            x[:] = rhs
+            x.copy_host_to_device()
+        else:
+            xv = _values_of(x)
+            xv[...] = rhs
+
+    def inertia_enabled(self):
+        return True
+
+    def get_inertia(self):
+        return self.ldl.get_inertia()
+
+    def set_pivot_tolerance(self, pivtol):
+        pass

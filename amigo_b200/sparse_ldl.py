@@ -274,6 +274,33 @@ class SparseLDL:
         _native.check(self._h, st, "node_pivots")
         return a, b
 
+    # -- profiling ---------------------------------------------------------------
+    PHASES = ("fronts", "big_assembly", "big_panel", "big_update", "solve_forward",
+              "solve_backward")
+
+    def set_profiling(self, on: bool):
+        self._lib.b200ldl_set_profiling(self._h, 1 if on else 0)
+
+    def reset_profile(self):
+        self._lib.b200ldl_reset_profile(self._h)
+
+    def launch_count(self) -> int:
+        return int(self._lib.b200ldl_launch_count(self._h))
+
+    def work(self) -> dict:
+        v = np.zeros(4)
+        self._lib.b200ldl_work(self._h, v.ctypes.data_as(_native._f64p), 4)
+        return {"flops": v[0], "panel_flops": v[1], "update_flops": v[2], "update_bytes": v[3]}
+
+    def profile(self) -> list:
+        """Per kernel class: device milliseconds (CUDA events), launches, and
+        the algorithmic work used for its roofline: flops for the front and
+        panel kernels (compute), bytes for the update and solve kernels."""
+        v = np.zeros(2 * len(self.PHASES))
+        self._lib.b200ldl_profile(self._h, v.ctypes.data_as(_native._f64p), len(v))
+        return [{"name": nm, "ms": float(v[2 * i]), "launches": int(v[2 * i + 1])}
+                for i, nm in enumerate(self.PHASES)]
+
     def stats(self) -> dict:
         v = np.zeros(6)
         st = self._lib.b200ldl_stats(self._h, v.ctypes.data_as(_native._f64p), 6)

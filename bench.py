@@ -1,0 +1,394 @@
+#!/usr/bin/env python
+"""KKT LDL^T factor+solve throughput on B200.
+
+Workload: the 256 x 256 plane-stress PDE-constrained KKT system
+(amigo_b200.workloads.plane_stress_kkt: n = 329,732, 6.09e6 nonzeros, five
+right-hand sides: a unit load plus four N(0,1) columns), AMD ordering, the
+reference solver's settings (ustab 0.01, pivot_tol 1e-14). One step = one
+numeric factorization + one 5-RHS solve; the symbolic analysis runs once per
+pattern outside the timed region, as in the interior-point loop.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). With N > 1 (torchrun) every rank factors its
+own replica (a single factorization does not shard), value = all ranks'
+steps / max-over-ranks time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "KKT LDLᵀ factor+solve/s at 1e-10 backward err: mixed-prec vs FP64, 1 B200"
+UNIT = "factor+solve/s"
+BERR_TARGET = 1e-10
+L2_BYTES = 126 * 1024 * 1024
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]),
+                "source": "measured"}
+    except Exception:
+        return dict(FALLBACK_PEAKS, source="fallback")
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region (median SM clock and the
+    throttle reasons seen)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.t is not None:
+            self.t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {
+            "sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": float(max(smax)) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def backward_error(system, x, b) -> float:
+    r = b - system.matvec(x)
+    kn = system.inf_norm()
+    num = np.abs(r).max(axis=0)
+    den = kn * np.abs(x).max(axis=0) + np.abs(b).max(axis=0)
+    return float(np.max(num / den))
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_sample(system, threads: int, budget_s: float, max_steps: int, warmup: int):
+    """Time the reference's own SparseLDL (compiled from its sources into
+    oracle/_ref) on the host: factor + 5-RHS solve of the same system."""
+    from oracle import ref
+
+    env_threads = str(threads)
+    os.environ["OMP_NUM_THREADS"] = env_threads
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    r = ref.RefLDL(system.rowp, system.cols, order=ref.ORDER_AMD, openmp=threads > 1)
+    for _ in range(warmup):
+        r.factor(system.vals, system.diag)
+        r.solve(system.rhs)
+    times = []
+    t_all = time.perf_counter()
+    x = None
+    while len(times) < max_steps:
+        t0 = time.perf_counter()
+        r.factor(system.vals, system.diag)
+        x = r.solve(system.rhs)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_all > budget_s:
+            break
+    inertia = r.inertia()
+    r.close()
+    return times, inertia, x
+
+
+def run_reference(args, world, rank):
+    """The reference arm: the reference's CPU SparseLDL with all host threads."""
+    if rank != 0:
+        return 0
+    from amigo_b200.workloads import plane_stress_kkt
+    from oracle import ref
+
+    if not ref.available(openmp=True):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/liboracle_ref_omp.so not built"}))
+        return 0
+    s = plane_stress_kkt(args.nel)
+    cores = os.cpu_count() or 1
+    budget = float(os.environ.get("REFERENCE_BUDGET_S", "150"))
+    times, inertia, x = cpu_reference_sample(s, cores, budget, args.steps, min(args.warmup, 1))
+    ms = 1e3 * float(np.mean(times))
+    value = 1e3 / ms
+    sample = (f"{len(times)} of {args.steps} requested factor+5-RHS solves of the full "
+              f"system (time budget {budget:.0f} s), after {min(args.warmup, 1)} warm-up")
+    berr = backward_error(s, x, s.rhs)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": world, "steps": len(times), "warmup": min(args.warmup, 1),
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"plane-stress KKT {args.nel}x{args.nel} (n={s.n}, nnz={s.nnz}), "
+                               "5 RHS, AMD", "nrhs": 5, "parallelism": "host OpenMP"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "inertia": list(inertia), "backward_error": berr,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from amigo_b200.sparse_ldl import CSRMat, OrderingType, SparseLDL, Vector
+    from amigo_b200.workloads import plane_stress_kkt
+
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+    s = plane_stress_kkt(args.nel)
+    nrhs = s.rhs.shape[1]
+    vals = torch.as_tensor(s.vals, device=dev)
+    diag = torch.as_tensor(s.diag, device=dev)
+    b = torch.as_tensor(np.ascontiguousarray(s.rhs.T), device=dev).t()  # column-major
+    x = torch.empty_like(b)
+    x = x.t().contiguous().t()
+    ldl = SparseLDL(CSRMat(s.n, s.n, s.rowp, s.cols, vals), order=OrderingType.AMD)
+    dvec = Vector(diag)
+
+    def step():
+        ldl.factor(dvec)
+        x.copy_(b)
+        ldl.solve(x)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    xh = x.cpu().numpy()
+    berr = backward_error(s, xh, s.rhs)
+    inertia = ldl.get_inertia()
+    stats = ldl.stats()
+    work = ldl.work()
+    ldl.set_profiling(True)
+    ldl.reset_profile()
+
+    stream = torch.cuda.current_stream(dev)
+    sampler = ClockSampler(local)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    launches0 = ldl.launch_count()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = ldl.launch_count() - launches0
+    if world > 1:
+        torch.distributed.barrier()
+    ms_total = e0.elapsed_time(e1)
+    prof = ldl.profile()
+    ldl.set_profiling(False)
+    t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * args.steps / (ms_max / 1e3)
+
+    # end to end through the public API with host buffers (pinned)
+    hv = torch.empty(s.nnz, dtype=torch.float64, pin_memory=True)
+    hd = torch.empty(s.n, dtype=torch.float64, pin_memory=True)
+    hx = torch.empty((nrhs, s.n), dtype=torch.float64, pin_memory=True)
+    hv.numpy()[:] = s.vals
+    hd.numpy()[:] = s.diag
+    host_ldl = SparseLDL(CSRMat(s.n, s.n, s.rowp, s.cols, hv.numpy()), order=OrderingType.AMD)
+    hvec = Vector(hd.numpy())
+    xf = hx.numpy().T  # n x nrhs, column-major view of pinned memory
+
+    def e2e_step():
+        host_ldl.factor(hvec)
+        xf[...] = s.rhs
+        host_ldl.solve(xf)
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        e2e_step()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    te = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = world * args.steps / (float(te.item()) / 1e3)
+    berr_e2e = backward_error(s, np.array(xf), s.rhs)
+    h2d = (s.nnz + s.n + s.n * nrhs) * 8
+    d2h = s.n * nrhs * 8
+    host_ldl.close()
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+
+    # roofline of the dominant kernel class: device time from CUDA events the
+    # library records on its stream around each class over the timed region;
+    # algorithmic work per step from the factorization's own counters
+    peaks = load_peaks()
+    algo = {
+        # dense partial factorizations outside the big-front path (flops)
+        "fronts": ("tensor", work["flops"] - work["panel_flops"] - work["update_flops"]),
+        "big_panel": ("tensor", work["panel_flops"]),
+        # rank-kw updates: trailing lower triangle read + written, panels read
+        "big_update": ("hbm", work["update_bytes"]),
+        # contribution blocks read into the fronts (bytes)
+        "big_assembly": ("hbm", stats["cb_bytes"]),
+        # every factor entry read once per sweep, plus the update vectors
+        "solve_forward": ("hbm", stats["L_bytes"]),
+        "solve_backward": ("hbm", stats["L_bytes"]),
+    }
+    for p_ in prof:
+        p_["bound"], w = algo[p_["name"]]
+        p_["work_per_step"] = w
+    dom = max(prof, key=lambda p_: p_["ms"])
+    per_launch_ms = dom["ms"] / max(1, dom["launches"])
+    total_work = dom["work_per_step"] * args.steps
+    if dom["bound"] == "hbm":
+        achieved = total_work / max(1e-12, dom["ms"] / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                "kernel": dom["name"], "launches": dom["launches"],
+                "ms_per_launch": per_launch_ms, "peak_source": peaks["source"]}
+    else:
+        achieved = total_work / max(1e-12, dom["ms"] / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"],
+                "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"], "traffic": None,
+                "kernel": dom["name"], "launches": dom["launches"],
+                "ms_per_launch": per_launch_ms, "peak_source": peaks["source"],
+                "note": "FP64 arithmetic measured against the bf16 dense peak"}
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import ref
+
+        if ref.available():
+            times, cinertia, _ = cpu_reference_sample(s, 1, 30.0, 1, 0)
+            cms = 1e3 * float(np.mean(times))
+            cpu = {"value": 1e3 / cms, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"{len(times)} factor+5-RHS solve of the full system, serial "
+                             "build, OPENBLAS_NUM_THREADS=1",
+                   "inertia": list(cinertia)}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {
+            "workload": f"plane-stress KKT {args.nel}x{args.nel} (n={s.n}, nnz={s.nnz}), "
+                        f"{nrhs} RHS, AMD ordering, FP64 factor+solve",
+            "nrhs": nrhs, "parallelism": "replicas" if world > 1 else "single GPU",
+            "l2": "inputs and per-step factor traffic larger than L2 (126 MB); no flush",
+        },
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "backward_error": berr_e2e},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "backward_error": berr,
+        "berr_target_met": bool(berr <= BERR_TARGET),
+        "inertia": list(inertia),
+        "expected_inertia": list(s.expected_inertia),
+        "factor_flops_executed": stats["flops"],
+        "max_front": stats["max_front"],
+        "delayed_pivots": stats["delayed"],
+        "profile": prof,
+    }
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--nel", type=int, default=256, help=argparse.SUPPRESS)
+    ap.add_argument("--no-cpu-baseline", action="store_true", help=argparse.SUPPRESS)
+    args = ap.parse_args(argv)
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+    return run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

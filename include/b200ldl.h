@@ -109,6 +109,24 @@ int b200ldl_node_pivots(b200ldl_t h, int* num_pivots, int* num_delayed);
  * delayed pivots summed over supernodes, stats[5] = number of levels. */
 int b200ldl_stats(b200ldl_t h, double* stats, int nstats);
 
+/* Profiling (no counterpart in the reference, which has no GPU timers):
+ * when enabled, CUDA events on the handle's stream time each kernel class.
+ * b200ldl_profile writes, for each class p in {fronts, big-front assembly,
+ * big-front panels, big-front trailing updates, forward solve, backward
+ * solve}, out[2p] = accumulated milliseconds and out[2p+1] = kernel
+ * launches since the last reset. */
+int b200ldl_set_profiling(b200ldl_t h, int enable);
+int b200ldl_reset_profile(b200ldl_t h);
+int b200ldl_profile(b200ldl_t h, double* out, int n);
+
+/* Kernels launched by this handle since creation. */
+long long b200ldl_launch_count(b200ldl_t h);
+
+/* Work of the last factorization: out[0] = flops executed in all fronts,
+ * out[1] = of which in big-front panels, out[2] = in big-front trailing
+ * updates, out[3] = bytes moved by the trailing updates. */
+int b200ldl_work(b200ldl_t h, double* out, int n);
+
 #ifdef __cplusplus
 }
 #endif
