@@ -99,6 +99,7 @@ struct b200ldl_handle {
   DevBuf<unsigned long long> d_used;
   DevBuf<BigFront> d_big;
   DevBuf<int> d_big_meta;
+  DevBuf<int> d_class_list;
   DevBuf<long long> d_tile_ptr;
   unsigned long long icap = 0, dcap = 0;
   DevState st{};
@@ -306,7 +307,8 @@ void upload_plan(b200ldl_t h) {
   CK(h->d_flops.alloc(4));
   CK(h->d_used.alloc(3));
   CK(h->d_big.alloc(nn));
-  CK(h->d_big_meta.alloc(8));
+  CK(h->d_big_meta.alloc(16));
+  CK(h->d_class_list.alloc((size_t)6 * std::max(1, nn)));
   CK(h->d_tile_ptr.alloc(nn + 1));
   h->uploaded = true;
 }
@@ -333,6 +335,8 @@ void bind_state(b200ldl_t h) {
   st.flops = h->d_flops.ptr;
   st.big = h->d_big.ptr;
   st.big_meta = h->d_big_meta.ptr;
+  st.class_list = h->d_class_list.ptr;
+  for (int c = 0; c < 5; c++) st.cf_limit[c] = cluster_front_limit(c);
   st.tile_ptr = h->d_tile_ptr.ptr;
 }
 
@@ -363,18 +367,29 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
     for (int l = 0; l < h->num_levels; l++) {
       const int b = h->level_ptr[l];
       const int cnt = h->level_ptr[l + 1] - b;
-      CK(cudaMemsetAsync(h->d_big_meta.ptr, 0, 8 * sizeof(int), h->stream));
+      CK(cudaMemsetAsync(h->d_big_meta.ptr, 0, 16 * sizeof(int), h->stream));
       h->prof.begin(h->stream);
       launch_factor_level(h->plan, h->st, h->d_level_nodes.ptr + b, cnt, prm, h->stream,
                           vals, diag);
       h->prof.end(kPhFront, h->stream, 1);
       CK(cudaGetLastError());
-      int meta[8];
-      CK(cudaMemcpyAsync(meta, h->d_big_meta.ptr, 8 * sizeof(int), cudaMemcpyDeviceToHost,
+      int meta[16];
+      CK(cudaMemcpyAsync(meta, h->d_big_meta.ptr, 16 * sizeof(int), cudaMemcpyDeviceToHost,
                          h->stream));
       CK(cudaStreamSynchronize(h->stream));
       if (meta[0] > 0) {
-        BigLevelInfo info{meta[0], meta[1], meta[2], meta[3], meta[4], meta[5]};
+        BigLevelInfo info{};
+        info.count = meta[0];
+        info.max_f = meta[1];
+        info.max_fs = meta[2];
+        info.count_large = meta[3];
+        info.max_fs_large = meta[4];
+        info.cluster_launches = 0;
+        for (int c = 0; c < 5; c++) {
+          info.class_count[c] = meta[5 + c];
+          info.class_maxf[c] = meta[10 + c];
+          if (meta[5 + c] > 0) info.cluster_launches++;
+        }
         CK(launch_big_level(h->plan, h->st, info, h->level_maxkids[l], prm, vals, diag,
                             h->stream, h->prof));
       }

@@ -87,8 +87,8 @@ __device__ void block_reduce(BlockRed& r, double& bv, int& bi, double& cm) {
 
 // ---------------------------------------------------------------- assembly
 
-__global__ void big_zero_kernel(DevState s) {
-  const BigFront& B = s.big[blockIdx.x];
+__global__ void big_zero_kernel(DevState s, const int* __restrict__ list) {
+  const BigFront& B = s.big[list[blockIdx.x]];
   double* F = s.dpool + B.doff;
   const int f = B.f;
   const int lane = threadIdx.x & 31;
@@ -101,8 +101,9 @@ __global__ void big_zero_kernel(DevState s) {
 }
 
 __global__ void big_scatter_kernel(DevPlan p, DevState s, const double* __restrict__ vals,
-                                   const double* __restrict__ diag) {
-  const BigFront& B = s.big[blockIdx.x];
+                                   const double* __restrict__ diag,
+                                   const int* __restrict__ list) {
+  const BigFront& B = s.big[list[blockIdx.x]];
   double* F = s.dpool + B.doff;
   const int f = B.f, ns = B.ns, nd_in = B.nd_in, node = B.node;
   const int64_t e0 = p.scat_ptr[node];
@@ -115,8 +116,9 @@ __global__ void big_scatter_kernel(DevPlan p, DevState s, const double* __restri
   }
 }
 
-__global__ void big_diag_kernel(DevPlan p, DevState s, const double* __restrict__ diag) {
-  const BigFront& B = s.big[blockIdx.x];
+__global__ void big_diag_kernel(DevPlan p, DevState s, const double* __restrict__ diag,
+                                const int* __restrict__ list) {
+  const BigFront& B = s.big[list[blockIdx.x]];
   double* F = s.dpool + B.doff;
   const int f = B.f;
   const int v0 = p.var_ptr[B.node];
@@ -125,8 +127,8 @@ __global__ void big_diag_kernel(DevPlan p, DevState s, const double* __restrict_
 }
 
 // extend-add of the c-th child of every big front
-__global__ void big_extend_kernel(DevPlan p, DevState s, int c) {
-  const BigFront& B = s.big[blockIdx.x];
+__global__ void big_extend_kernel(DevPlan p, DevState s, int c, const int* __restrict__ list) {
+  const BigFront& B = s.big[list[blockIdx.x]];
   const int node = B.node;
   const int kb = p.kid_ptr[node];
   const int ke = p.kid_ptr[node + 1];
@@ -254,16 +256,14 @@ __device__ __forceinline__ void push_part(cg::cluster_group& cl, Part* slots, in
   if (threadIdx.x < CL) *cl.map_shared_rank(slots + rank, (unsigned)threadIdx.x) = p;
 }
 
-// FUSED (with CL == 1): one CTA factors a medium front completely in one
-// launch, alternating panels (in shared memory) and its own trailing update
-// from those panels. Otherwise one panel per launch, the trailing update
-// follows in big_update_kernel.
-template <int CL, bool FUSED>
+// One panel per launch for every front of the large class (the list
+// `list`); the trailing update follows in big_update_kernel.
+template <int CL>
 __global__ void __launch_bounds__(kPanelThreads)
-    big_panel_kernel(DevState s, FactorParams prm, int NB_arg, int smem_bytes) {
+    big_panel_kernel(DevState s, FactorParams prm, int NB, const int* __restrict__ list) {
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
-  BigFront* B = s.big + blockIdx.x / CL;
+  BigFront* B = s.big + list[blockIdx.x / CL];
   extern __shared__ __align__(16) double sm[];
   __shared__ Part slotA[CL], slotB[CL];
   __shared__ BlockRed red;
@@ -272,14 +272,6 @@ __global__ void __launch_bounds__(kPanelThreads)
   const int tid = threadIdx.x;
   if (B->state != 0) return;  // same value in every CTA of the cluster
   const int f = B->f;
-  if (FUSED != (f <= kMediumMax)) return;  // the other path owns this front
-  int NB = NB_arg;
-  if (FUSED) {
-    // widest panel whose rows fit in the launch's shared memory
-    NB = kBigPanelMax;
-    while (NB > 4 && (size_t)f * (2 * (NB + 1) + 2) * sizeof(double) > (size_t)smem_bytes)
-      NB >>= 1;
-  }
   const bool root = (B->nc == 0);
   int k = B->k;
   int ncand = B->ncand;
@@ -299,9 +291,9 @@ __global__ void __launch_bounds__(kPanelThreads)
   int kstart = k;
   int kw = 0;
   int npos = 0, nneg = 0;
-  double flops = 0.0, uflops = 0.0;
+  double flops = 0.0;
 
-  for (;;) {  // panels (more than one only when FUSED)
+  {  // one panel
   kstart = k;
   kw = 0;
   while (kw < NB - 1 && k < ncand) {
@@ -525,34 +517,7 @@ __global__ void __launch_bounds__(kPanelThreads)
     cl.sync();  // B4: new panel columns visible
   }
 
-  if constexpr (FUSED) {
-    // trailing update F(i,j) -= sum_c Lp(i,c) Wp(j,c), k <= j <= i < f, by
-    // this CTA with both panels in shared memory
-    if (kw > 0) {
-      __syncthreads();
-      const int lane = tid & 31;
-      const int warp = tid >> 5;
-      for (int j = k + warp; j < f; j += kPWarps) {
-        const double* wj = Wp + (size_t)j * NBP;
-        double* Fj = F + (size_t)f * j;
-        for (int i = j + lane; i < f; i += 32) {
-          const double* li = Lp + (size_t)i * NBP;
-          double acc = 0.0;
-          for (int c = 0; c < kw; c++) acc = fma(li[c], wj[c], acc);
-          Fj[i] -= acc;
-        }
-      }
-      if (tid == 0) {
-        const double r = (double)(f - k);
-        const double fl = r * (r + 1.0) * kw;
-        uflops += fl;
-        atomicAdd(s.flops + 2, fl);
-        atomicAdd(s.flops + 3, 8.0 * r * (r + 1.0));
-      }
-      __syncthreads();
-    }
-    if (k < ncand) continue;
-  } else {
+  {
     // W columns of the panel for the trailing update (rows >= k)
     for (int j = 0; j < kw; j++) {
       const int lo2 = max(r0, k);
@@ -560,21 +525,17 @@ __global__ void __launch_bounds__(kPanelThreads)
         Wg[(size_t)j * f + i] = Wp[(size_t)(i - r0) * NBP + j];
     }
   }
-  break;
-  }  // panels
+  }  // one panel
   if (rank == 0 && tid == 0) {
     B->k = k;
     B->ncand = ncand;
     B->kstart = kstart;
-    B->kw = FUSED ? 0 : kw;
+    B->kw = kw;
     B->npos += npos;
     B->nneg += nneg;
-    B->flops += flops + uflops;
+    B->flops += flops;
     atomicAdd(s.flops + 1, flops);
-    if (FUSED)
-      B->state = 2;
-    else if (k >= ncand)
-      B->state = 1;
+    if (k >= ncand) B->state = 1;
   }
 }
 
@@ -716,8 +677,13 @@ __global__ void big_finalize_kernel(DevState s, int nbig, int cholesky) {
   s.fv_off[node] = B.ioff;
   s.L_off[node] = B.doff;
   s.L_ld[node] = B.f;
-  s.cb_off[node] = B.doff + (long long)npiv * (B.f + 1);
-  s.cb_ld[node] = B.f;
+  if (B.pad == 1) {  // factored on chip: contribution block after L, ld m
+    s.cb_off[node] = B.doff + (long long)B.f * npiv;
+    s.cb_ld[node] = m > 0 ? m : 1;
+  } else {  // factored in place in the pool
+    s.cb_off[node] = B.doff + (long long)npiv * (B.f + 1);
+    s.cb_ld[node] = B.f;
+  }
   s.u_off[node] = (long long)atomicAdd(s.used + 2, (unsigned long long)m);
   if (!cholesky) {
     atomicAdd(s.inertia, B.npos);
@@ -726,9 +692,9 @@ __global__ void big_finalize_kernel(DevState s, int nbig, int cholesky) {
   atomicAdd(s.flops, B.flops);
 }
 
-template <int CL, bool FUSED>
+template <int CL>
 cudaError_t launch_panel(const DevState& s, const FactorParams& prm, int count, int NB,
-                         size_t smem, cudaStream_t stream) {
+                         size_t smem, const int* list, cudaStream_t stream) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(count * CL, 1, 1);
   cfg.blockDim = dim3(kPanelThreads, 1, 1);
@@ -741,7 +707,7 @@ cudaError_t launch_panel(const DevState& s, const FactorParams& prm, int count, 
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, big_panel_kernel<CL, FUSED>, s, prm, NB, (int)smem);
+  return cudaLaunchKernelEx(&cfg, big_panel_kernel<CL>, s, prm, NB, list);
 }
 
 constexpr size_t kPanelSmemMax = 224 * 1024;
@@ -750,20 +716,16 @@ constexpr size_t kPanelSmemMax = 224 * 1024;
 
 cudaError_t configure_big_kernels() {
   cudaError_t e;
-  e = cudaFuncSetAttribute(big_panel_kernel<1, true>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax);
+  e = cudaFuncSetAttribute(big_panel_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kPanelSmemMax);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(big_panel_kernel<4, false>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax);
+  e = cudaFuncSetAttribute(big_panel_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kPanelSmemMax);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(big_panel_kernel<8, false>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax);
+  e = cudaFuncSetAttribute(big_panel_kernel<16>,
+                           cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(big_panel_kernel<16, false>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPanelSmemMax);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(big_panel_kernel<16, false>,
-                              cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  return configure_cluster_front_kernels();
 }
 
 cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
@@ -774,45 +736,48 @@ cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevel
   const int cols_per = 8;  // warps per CTA in the assembly kernels
   const int ychunks = std::min(256, (info.max_f + cols_per - 1) / cols_per);
   prof.begin(stream);
-  big_zero_kernel<<<dim3(nb, ychunks), 256, 0, stream>>>(s);
-  big_scatter_kernel<<<dim3(nb, 16), 256, 0, stream>>>(p, s, vals, diag);
-  if (diag) big_diag_kernel<<<nb, 256, 0, stream>>>(p, s, diag);
-  for (int c = 0; c < maxkids; c++)
-    big_extend_kernel<<<dim3(nb, ychunks), 256, 0, stream>>>(p, s, c);
-  prof.end(kPhBigAsm, stream, 2 + (diag ? 1 : 0) + maxkids);
 
-  // medium fronts: one CTA each, whole factorization in one launch
-  if (info.max_f_medium > 0) {
-    size_t msmem = (size_t)info.max_f_medium * (2 * (16 + 1) + 2) * sizeof(double);
-    if (msmem > kPanelSmemMax) msmem = kPanelSmemMax;
-    prof.begin(stream);
-    cudaError_t e = launch_panel<1, true>(s, prm, nb, 16, msmem, stream);
+  // fronts that fit in a cluster's distributed shared memory
+  {
+    cudaError_t e = launch_cluster_fronts(p, s, info.class_count, info.class_maxf, vals, diag,
+                                          prm, stream, p.num_nodes);
     if (e != cudaSuccess) return e;
-    prof.end(kPhBigPanel, stream, 1);
   }
+  prof.end(kPhBigPanel, stream, info.cluster_launches);
   if (info.count_large == 0) {
     prof.begin(stream);
     big_finalize_kernel<<<(nb + 255) / 256, 256, 0, stream>>>(s, nb, prm.cholesky);
     prof.end(kPhBigAsm, stream, 1);
     return cudaGetLastError();
   }
-  // large fronts: a cluster per front and a panel per launch. Cluster size
-  // and panel width from the largest front: aim for <= 200 rows per CTA so
-  // that two CTAs fit on an SM.
+  // larger fronts: a cluster per front, one panel per launch over the front
+  // in global memory; <= 200 rows per CTA where possible
+  const int* list5 = s.class_list + (size_t)5 * p.num_nodes;
   int CL = info.max_f > 1600 ? 16 : 8;
   const int R = (info.max_f + CL - 1) / CL;
   int NB = kBigPanelMax;
   while (NB > 4 && (size_t)R * (2 * (NB + 1) + 2) * sizeof(double) > kPanelSmemMax) NB >>= 1;
   const size_t smem = (size_t)R * (2 * (NB + 1) + 2) * sizeof(double);
   const int steps = (info.max_fs_large + (NB - 2)) / (NB - 1) + 1;
+  {
+    const int nl = info.count_large;
+    const int ych = std::min(256, (info.max_f + 7) / 8);
+    prof.begin(stream);
+    big_zero_kernel<<<dim3(nl, ych), 256, 0, stream>>>(s, list5);
+    big_scatter_kernel<<<dim3(nl, 16), 256, 0, stream>>>(p, s, vals, diag, list5);
+    if (diag) big_diag_kernel<<<nl, 256, 0, stream>>>(p, s, diag, list5);
+    for (int c = 0; c < maxkids; c++)
+      big_extend_kernel<<<dim3(nl, ych), 256, 0, stream>>>(p, s, c, list5);
+    prof.end(kPhBigAsm, stream, 2 + (diag ? 1 : 0) + maxkids);
+  }
   const int upd_grid = 148 * 4;
   for (int st = 0; st < steps; st++) {
     cudaError_t e;
     prof.begin(stream);
     if (CL == 16)
-      e = launch_panel<16, false>(s, prm, nb, NB, smem, stream);
+      e = launch_panel<16>(s, prm, info.count_large, NB, smem, list5, stream);
     else
-      e = launch_panel<8, false>(s, prm, nb, NB, smem, stream);
+      e = launch_panel<8>(s, prm, info.count_large, NB, smem, list5, stream);
     if (e != cudaSuccess) return e;
     prof.end(kPhBigPanel, stream, 1);
     prof.begin(stream);

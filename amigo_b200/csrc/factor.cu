@@ -188,11 +188,17 @@ __global__ void __launch_bounds__(kFactorThreads)
       const int slot = atomicAdd(s.big_meta, 1);
       atomicMax(s.big_meta + 1, f);
       atomicMax(s.big_meta + 2, fs);
-      if (f > kMediumMax) {
-        atomicAdd(s.big_meta + 3, 1);
+      int cls = 5;
+      for (int c = 4; c >= 0; c--)
+        if (f <= s.cf_limit[c]) cls = c;
+      if (cls == 5) {
+        const int q = atomicAdd(s.big_meta + 3, 1);
         atomicMax(s.big_meta + 4, fs);
+        s.class_list[(size_t)5 * p.num_nodes + q] = slot;
       } else {
-        atomicMax(s.big_meta + 5, f);
+        const int q = atomicAdd(s.big_meta + 5 + cls, 1);
+        atomicMax(s.big_meta + 10 + cls, f);
+        s.class_list[(size_t)cls * p.num_nodes + q] = slot;
       }
       BigFront b;
       b.node = node;

@@ -134,7 +134,10 @@ struct DevState {
   double* flops;    // [4] executed flops: [0] all fronts, [1] big panels,
                     // [2] big trailing updates, [3] trailing-update bytes moved
   BigFront* big;    // [nn] big fronts of the current level
-  int* big_meta;    // [4]: count, max f, max fs, unused
+  int* big_meta;    // [16]: count, max f, max fs, count large, max fs large,
+                    // class counts [5..9], class max f [10..14]
+  int* class_list;  // [6][nn] big-front indices per size class
+  int cf_limit[5];  // largest front of each on-chip class
   long long* tile_ptr;  // [nn+1] update tiles per big front (prefix)
 };
 
@@ -159,12 +162,20 @@ size_t factor_smem_bytes();
 // number of children among the level's supernodes.
 struct BigLevelInfo {
   int count, max_f, max_fs;
-  int count_large, max_fs_large, max_f_medium;
+  int count_large, max_fs_large;
+  int class_count[5], class_maxf[5];
+  int cluster_launches;
 };
 
-// Fronts above kSmemFrontMax and up to kMediumMax are factored by one CTA in
-// a single launch; larger ones by a thread-block cluster per panel.
-constexpr int kMediumMax = 768;
+// Fronts above kSmemFrontMax are factored on chip by a cluster of 1, 2, 4,
+// 8 or 16 CTAs (class 0..4) when they fit in its distributed shared memory
+// (cluster_front_limit(class)); larger ones (class 5) panel by panel from
+// global memory.
+int cluster_front_limit(int cl_index);
+cudaError_t configure_cluster_front_kernels();
+cudaError_t launch_cluster_fronts(const DevPlan& p, const DevState& s, const int* counts,
+                                  const int* maxf, const double* vals, const double* diag,
+                                  const FactorParams& prm, cudaStream_t stream, int nn);
 cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
                              int maxkids, const FactorParams& prm, const double* vals,
                              const double* diag, cudaStream_t stream, Prof& prof);
