@@ -127,6 +127,24 @@ long long b200ldl_launch_count(b200ldl_t h);
  * updates, out[3] = bytes moved by the trailing updates. */
 int b200ldl_work(b200ldl_t h, double* out, int n);
 
+/* Allocation-free dense solve (no counterpart in the reference; the
+ * reference always allocates its factor storage). For callers that must not
+ * allocate device memory while running, e.g. a real-time loop re-solving a
+ * small KKT system, or a plugin in a process whose framework has reserved
+ * the device memory. Factors the dense symmetric matrix a (n x n,
+ * column-major, lower triangle read, leading dimension lda) with
+ * Bunch-Kaufman LDL^T and overwrites b (n x nrhs, ldb) with the solution;
+ * inertia (npos, nneg) goes to inertia[0..1] if not NULL. All pointers are
+ * DEVICE pointers; stream is a cudaStream_t (NULL = default stream); the
+ * call is asynchronous. Scratch is a fixed device array inside the library:
+ * n must be <= 512 (status -6 otherwise), every GPU that loads the library
+ * holds the array (2 MiB) until exit, all calls share it, and calls whose
+ * kernels overlap on the GPU race on it (order them on one stream). The
+ * first call on a device looks up the array's address; make it before any
+ * stream capture. Calls no cudaMalloc/cudaFree or allocating routine. */
+int b200ldl_dense_solve_noalloc(int n, const double* a, int lda, double* b,
+                                int ldb, int nrhs, int* inertia, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
