@@ -28,6 +28,9 @@ SIGNATURES = {
     "b200ldl_factor_host": (ctypes.c_int, [_vp, _f64p, _f64p]),
     "b200ldl_solve": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
     "b200ldl_solve_host": (ctypes.c_int, [_vp, ctypes.c_int, _f64p, ctypes.c_int]),
+    "b200ldl_solve_refine": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp,
+                                            ctypes.c_int, ctypes.c_int, ctypes.c_double, _f64p,
+                                            _i32p]),
     "b200ldl_get_inertia": (ctypes.c_int, [_vp, _i32p, _i32p]),
     "b200ldl_last_error": (ctypes.c_char_p, [_vp]),
     "b200ldl_symbolic_sizes": (ctypes.c_int, [_vp, _i32p, _i32p]),

@@ -76,6 +76,9 @@ struct b200ldl_handle {
 
   Symbolic sym;
   bool uploaded = false;
+  std::vector<int> h_rowp, h_cols;  // the pattern, for residuals
+  DevBuf<int> d_rowp, d_cols;
+  DevBuf<double> d_refine, d_norms;
   // host copies of the plan (uploaded lazily on the first factorization so
   // that the symbolic phase runs on machines without a GPU)
   std::vector<int> hp_ns, hp_nc, hp_kid_ptr, hp_kids, hp_cmap, hp_scat_csr, hp_scat_row,
@@ -112,7 +115,7 @@ struct b200ldl_handle {
   int fmax = 0;
   std::vector<int> level_fmax;
   Prof prof;
-  double flops4[4] = {0, 0, 0, 0};
+  double flops4[kWork] = {};
   double sum_delayed = 0.0;
 };
 
@@ -273,6 +276,8 @@ void upload_plan(b200ldl_t h) {
   CK(h->d_scat_row.upload(h->hp_scat_row));
   CK(h->d_scat_col.upload(h->hp_scat_col));
   CK(h->d_level_nodes.upload(h->hp_level_nodes));
+  CK(h->d_rowp.upload(h->h_rowp));
+  CK(h->d_cols.upload(h->h_cols));
 
   DevPlan& p = h->plan;
   p.n = s.n;
@@ -304,7 +309,7 @@ void upload_plan(b200ldl_t h) {
   CK(h->d_u_off.alloc(nn));
   CK(h->d_err.alloc(4));
   CK(h->d_inertia.alloc(2));
-  CK(h->d_flops.alloc(4));
+  CK(h->d_flops.alloc(kWork));
   CK(h->d_used.alloc(3));
   CK(h->d_big.alloc(nn));
   CK(h->d_big_meta.alloc(16));
@@ -362,7 +367,7 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
     CK(cudaMemsetAsync(h->d_err.ptr, 0, sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_err.ptr + 1, 0xff, sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_inertia.ptr, 0, 2 * sizeof(int), h->stream));
-    CK(cudaMemsetAsync(h->d_flops.ptr, 0, 4 * sizeof(double), h->stream));
+    CK(cudaMemsetAsync(h->d_flops.ptr, 0, kWork * sizeof(double), h->stream));
     CK(cudaMemsetAsync(h->d_ndel.ptr, 0, sizeof(int) * std::max(1, h->sym.num_nodes), h->stream));
     for (int l = 0; l < h->num_levels; l++) {
       const int b = h->level_ptr[l];
@@ -401,7 +406,8 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
                        cudaMemcpyDeviceToHost, h->stream));
     CK(cudaMemcpyAsync(h->inertia, h->d_inertia.ptr, 2 * sizeof(int), cudaMemcpyDeviceToHost,
                        h->stream));
-    CK(cudaMemcpyAsync(h->flops4, h->d_flops.ptr, 4 * sizeof(double), cudaMemcpyDeviceToHost,
+    CK(cudaMemcpyAsync(h->flops4, h->d_flops.ptr, kWork * sizeof(double),
+                       cudaMemcpyDeviceToHost,
                        h->stream));
     CK(cudaStreamSynchronize(h->stream));
     h->exec_flops = h->flops4[0];
@@ -503,6 +509,8 @@ int b200ldl_create(b200ldl_t* out, int n, int nnz, const int* rowp, const int* c
   int st = guarded(h.get(), [&]() {
     h->sym = analyze(static_cast<Ordering>(order), n, rowp, cols);
     build_plan(h.get(), rowp, cols);
+    h->h_rowp.assign(rowp, rowp + n + 1);
+    h->h_cols.assign(cols, cols + nnz);
     return 0;
   });
   if (st != 0) {
@@ -648,6 +656,65 @@ int b200ldl_stats(b200ldl_t h, double* stats, int nstats) {
   });
 }
 
+int b200ldl_solve_refine(b200ldl_t h, const double* vals, const double* diag, int nrhs,
+                         const double* b, int ldb, double* x, int ldx, int max_iter, double tol,
+                         double* berr_out, int* iters_out) {
+  return guarded(h, [&]() {
+    if (!h->factored) return fail(h, -5, "solve called before a successful factor");
+    if (nrhs < 0 || ldb < h->n || ldx < h->n || max_iter < 0 || (nrhs > 0 && (!b || !x)) ||
+        (h->nnz > 0 && !vals))
+      return fail(h, -1, "bad refine arguments");
+    if (iters_out) *iters_out = 0;
+    if (nrhs == 0 || h->n == 0) return 0;
+    const int n = h->n;
+    const int chunk = refine_max_rhs();
+    if (h->d_refine.count < (size_t)n * chunk) CK(h->d_refine.alloc((size_t)n * chunk));
+    if (h->d_norms.count < (size_t)(1 + 3 * chunk)) CK(h->d_norms.alloc(1 + 3 * chunk));
+    double* r = h->d_refine.ptr;
+    double* nrm = h->d_norms.ptr;  // [0] ||K||, [1..] ||b||, ||x||, ||r|| per column
+    CK(cudaMemsetAsync(nrm, 0, sizeof(double), h->stream));
+    launch_infnorm(n, h->d_rowp.ptr, h->d_cols.ptr, vals, diag, nrm, h->stream);
+    int max_it_done = 0;
+    for (int c0 = 0; c0 < nrhs; c0 += chunk) {
+      const int nr = std::min(chunk, nrhs - c0);
+      const double* bc = b + (size_t)ldb * c0;
+      double* xc = x + (size_t)ldx * c0;
+      launch_copy_cols(n, nr, bc, ldb, xc, ldx, h->stream);
+      run_solve(h, nr, xc, ldx);
+      CK(cudaMemsetAsync(nrm + 1, 0, sizeof(double) * chunk, h->stream));
+      launch_colmax(n, bc, ldb, nr, nrm + 1, h->stream);
+      int it = 0;
+      for (;; it++) {
+        launch_residual(n, h->d_rowp.ptr, h->d_cols.ptr, vals, diag, xc, ldx, bc, ldb, r, n, nr,
+                        h->stream);
+        CK(cudaMemsetAsync(nrm + 1 + chunk, 0, sizeof(double) * 2 * chunk, h->stream));
+        launch_colmax(n, xc, ldx, nr, nrm + 1 + chunk, h->stream);
+        launch_colmax(n, r, n, nr, nrm + 1 + 2 * chunk, h->stream);
+        double hn[1 + 3 * 8];
+        CK(cudaMemcpyAsync(hn, nrm, sizeof(double) * (1 + 3 * chunk), cudaMemcpyDeviceToHost,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        bool ok = true;
+        for (int c = 0; c < nr; c++) {
+          const double den = hn[0] * hn[1 + chunk + c] + hn[1 + c];
+          const double be = den > 0.0 ? hn[1 + 2 * chunk + c] / den : 0.0;
+          if (berr_out) berr_out[c0 + c] = be;
+          if (!(be <= tol)) ok = false;
+        }
+        if (ok || it >= max_iter) break;
+        run_solve(h, nr, r, n);
+        launch_axpy(n, nr, r, n, xc, ldx, h->stream);
+      }
+      max_it_done = std::max(max_it_done, it);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    h->prof.collect();
+    if (iters_out) *iters_out = max_it_done;
+    return 0;
+  });
+}
+
 int b200ldl_set_profiling(b200ldl_t h, int enable) {
   if (!h) return -1;
   h->prof.on = enable != 0;
@@ -673,7 +740,7 @@ long long b200ldl_launch_count(b200ldl_t h) { return h ? h->prof.total_launches 
 
 int b200ldl_work(b200ldl_t h, double* out, int n) {
   if (!h || !out) return -1;
-  for (int i = 0; i < 4 && i < n; i++) out[i] = h->flops4[i];
+  for (int i = 0; i < kWork && i < n; i++) out[i] = h->flops4[i];
   return 0;
 }
 

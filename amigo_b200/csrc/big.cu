@@ -743,7 +743,7 @@ cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevel
                                           prm, stream, p.num_nodes);
     if (e != cudaSuccess) return e;
   }
-  prof.end(kPhBigPanel, stream, info.cluster_launches);
+  prof.end(kPhCluster, stream, info.cluster_launches);
   if (info.count_large == 0) {
     prof.begin(stream);
     big_finalize_kernel<<<(nb + 255) / 256, 256, 0, stream>>>(s, nb, prm.cholesky);

@@ -1,21 +1,41 @@
 // Fronts resident in a thread-block cluster's distributed shared memory.
 //
-// A front of size f (145 <= f <= kClusterFrontMax) is held entirely on chip:
-// its lower triangle is split row-cyclically over the CL CTAs of a cluster
-// (row i on CTA i % CL, rows stored packed, row-major), so every CTA holds
-// about f^2 / (2 CL) doubles and the work per CTA is balanced. The front is
-// assembled straight into DSMEM (CSR entries, the diagonal vector, the
-// children's contribution blocks), factored right-looking with the
-// reference's threshold 1x1 / 2x2 / delay tests (SparseLDL::
-// factor_front_matrix_block, include/sparse_ldl.h:1316-1553; Bunch-Kaufman
-// when there are no contribution rows, as LAPACK dsytrf there), and only the
-// factor columns and the contribution block leave the chip.
+// A front of size f (145 <= f <= cluster_front_limit(4)) is held entirely on
+// chip: its lower triangle is split row-cyclically over the CL CTAs of a
+// cluster (physical row r on CTA r % CL, rows stored packed, row-major), so
+// every CTA holds about f^2 / (2 CL) doubles. The front is assembled
+// straight into DSMEM (CSR entries, the diagonal vector, the children's
+// contribution blocks), factored with the reference's threshold 1x1 / 2x2 /
+// delay tests (SparseLDL::factor_front_matrix_block,
+// include/sparse_ldl.h:1316-1553; Bunch-Kaufman when there are no
+// contribution rows, as LAPACK dsytrf there), and only the factor columns
+// and the contribution block leave the chip.
 //
-// Per accepted 1x1 pivot: every CTA reduces the pivot column over its rows,
-// pushes its partial into every CTA's slot through DSMEM, one cluster
-// barrier, every thread reduces the slots (identical decisions everywhere),
-// each CTA gathers the pivot column from its owners and applies the rank-1
-// update to its own rows. No global memory is touched inside the loop.
+// Symmetric interchanges are never carried out on the data. The logical
+// order of the front (what the reference's symm_swap produces) is kept as a
+// permutation perm / ipos replicated in every CTA, and element {i, j} is
+// read from the physical lower-triangle slot of {perm[i], perm[j]}. A delay
+// or a pivot interchange is a two-entry update of perm. The factor columns
+// and the contribution block are written out in logical order at the end.
+//
+// Speculative delay chains. A delay leaves the Schur complement unchanged,
+// so the candidates the reference would test after t delays in a row
+// (position k, then the ones swapped in from ncand-1, ncand-2, ...) are
+// known in advance and have the same columns. Each step therefore forms the
+// columns of a chain of up to 8 candidates at once (one per warp), reduces
+// their statistics in one cluster exchange, forms the imax columns the
+// tests need in a second exchange, and then replays the reference's
+// sequential decisions on those values: the first member that is accepted
+// ends the chain, the ones before it are delayed. The decisions are the
+// ones the one-candidate-at-a-time algorithm takes.
+//
+// Blocked: accepted pivot columns are collected in panels of up to 16.
+// Inside a panel the front is left untouched: a candidate column is
+// F(:,c) - Lp W(c,:)^T with the panel's L on the owner's rows and a copy of
+// the panel's W rows in every CTA (the reference's W formulation,
+// sparse_ldl.h:1337-1344). After the panel each CTA applies one
+// register-tiled rank-kw update to its own remaining rows from its own
+// shared memory.
 #include <cooperative_groups.h>
 
 #include <climits>
@@ -30,21 +50,11 @@ namespace {
 
 constexpr int kCfThreads = 256;
 constexpr int kCfWarps = kCfThreads / 32;
+constexpr int kNB = 16;           // panel width (pivot columns per trailing update)
+constexpr int kNBP = kNB + 1;     // odd row stride of the panel arrays
+constexpr int kChain = kCfWarps;  // candidates evaluated per step, one per warp
 
-struct CfPart {
-  double v;
-  int i;
-  int pad;
-  double m;
-  double x;
-  double y;
-};
-
-struct CfRed {
-  double v[kCfWarps];
-  int i[kCfWarps];
-  double m[kCfWarps];
-};
+enum : int { kDelay = 0, kOne = 1, kTwo = 2, kNeedRow = 3, kZero = 4, kOneImax = 5 };
 
 __device__ __forceinline__ void keep_larger(double& bv, int& bi, double v, int i) {
   if (v > bv || (v == bv && i < bi)) {
@@ -53,48 +63,13 @@ __device__ __forceinline__ void keep_larger(double& bv, int& bi, double v, int i
   }
 }
 
-__device__ void cf_reduce(CfRed& r, double& bv, int& bi, double& cm) {
-  const int lane = threadIdx.x & 31;
-  const int w = threadIdx.x >> 5;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const double ov = __shfl_down_sync(0xffffffffu, bv, o);
-    const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-    const double om = __shfl_down_sync(0xffffffffu, cm, o);
-    keep_larger(bv, bi, ov, oi);
-    cm = fmax(cm, om);
-  }
-  if (lane == 0) {
-    r.v[w] = bv;
-    r.i[w] = bi;
-    r.m[w] = cm;
-  }
-  __syncthreads();
-  bv = r.v[0];
-  bi = r.i[0];
-  cm = r.m[0];
-#pragma unroll
-  for (int q = 1; q < kCfWarps; q++) {
-    keep_larger(bv, bi, r.v[q], r.i[q]);
-    cm = fmax(cm, r.m[q]);
-  }
-  __syncthreads();
-}
-
-// offset of row i inside its owner's packed storage (owner i % CL, local
-// row q = i / CL): q (r + 1) + CL q (q - 1) / 2
+// offset of physical row r inside its owner's packed storage (owner r % CL,
+// local row q = r / CL): q (o + 1) + CL q (q - 1) / 2 with o = r % CL
 template <int CL>
-__device__ __forceinline__ long long row_off(int i) {
-  const long long q = i / CL;
-  const long long r = i - q * CL;
-  return q * (r + 1) + (long long)CL * q * (q - 1) / 2;
-}
-
-template <int CL>
-__device__ __forceinline__ double* row_ptr(cg::cluster_group& cl, double* tri, int rank, int i) {
-  const int o = i % CL;
-  double* base = (o == rank) ? tri : cl.map_shared_rank(tri, o);
-  return base + row_off<CL>(i);
+__host__ __device__ __forceinline__ long long row_off(int r) {
+  const long long q = r / CL;
+  const long long o = r - q * CL;
+  return q * (o + 1) + (long long)CL * q * (q - 1) / 2;
 }
 
 // packed length of CTA `rank`'s rows for a front of size f
@@ -104,70 +79,112 @@ __host__ __device__ __forceinline__ long long tri_len(int f, int rank) {
   return Q * (rank + 1) + (long long)CL * Q * (Q - 1) / 2;
 }
 
-template <int CL>
-__device__ __forceinline__ void push(cg::cluster_group& cl, CfPart* slots, int rank,
-                                     const CfPart& p) {
-  if (threadIdx.x < CL) *cl.map_shared_rank(slots + rank, (unsigned)threadIdx.x) = p;
-}
-
-// symmetric interchange of rows/columns a < b of the distributed triangle;
-// every element pair is exchanged by exactly one thread of the cluster
-template <int CL>
-__device__ void tri_swap(cg::cluster_group& cl, double* tri, int rank, int f, int a, int b,
-                         int* fv, int* orig) {
-  const int n1 = a;
-  const int n2 = b - a - 1;
-  const int n3 = f - b - 1;
-  const int total = n1 + 1 + n2 + n3;
-  double* ra = row_ptr<CL>(cl, tri, rank, a);
-  double* rb = row_ptr<CL>(cl, tri, rank, b);
-  for (int t = rank * blockDim.x + threadIdx.x; t < total; t += CL * blockDim.x) {
-    double *p, *q;
-    if (t < n1) {
-      p = ra + t;
-      q = rb + t;
-    } else if (t == n1) {
-      p = ra + a;
-      q = rb + b;
-    } else if (t < n1 + 1 + n2) {
-      const int j = a + 1 + (t - n1 - 1);
-      p = row_ptr<CL>(cl, tri, rank, j) + a;
-      q = rb + j;
-    } else {
-      const int j = b + 1 + (t - n1 - 1 - n2);
-      double* rj = row_ptr<CL>(cl, tri, rank, j);
-      p = rj + a;
-      q = rj + b;
-    }
-    const double tmp = *p;
-    *p = *q;
-    *q = tmp;
-  }
-  if (rank == 0 && threadIdx.x == 0) {
-    int t = fv[a];
-    fv[a] = fv[b];
-    fv[b] = t;
-    t = orig[a];
-    orig[a] = orig[b];
-    orig[b] = t;
+// the same shared-memory object in CTA r of the cluster
+template <int CL, typename T>
+__device__ __forceinline__ T* at_rank(cg::cluster_group& cl, T* ptr, int r, int rank) {
+  if constexpr (CL == 1) {
+    return ptr;
+  } else {
+    return (r == rank) ? ptr : cl.map_shared_rank(ptr, (unsigned)r);
   }
 }
 
-enum : int { kDelay = 0, kOne = 1, kTwo = 2, kNeedRow = 3, kZero = 4 };
+template <int CL>
+__device__ __forceinline__ double* row_ptr(cg::cluster_group& cl, double* tri, int rank, int r) {
+  return at_rank<CL>(cl, tri, r % CL, rank) + row_off<CL>(r);
+}
+
+template <int CL>
+__device__ __forceinline__ void csync(cg::cluster_group& cl) {
+  if constexpr (CL == 1)
+    __syncthreads();
+  else
+    cl.sync();
+}
+
+// statistics of one candidate column over one CTA's rows outside the chain
+struct ColStat {
+  double bv;  // largest |.| among candidate rows
+  double cm;  // largest |.| among non-candidate rows
+  int bi;     // logical position of bv (smallest on ties)
+  int pad;
+};
+
+// what one chain member's tests need, reduced over the cluster
+struct Cand {
+  double wkk, abswik, colmax;  // pivot, best candidate entry, column max
+  double rmax, wii, wik;       // imax column: max off-diagonal, diagonal, entry at k
+  int dec1;                    // kOne / kZero / kNeedRow / kDelay from the column alone
+  int dec2;                    // kOne / kOneImax / kTwo / kDelay after the imax column
+  int imaxp;                   // imax: physical row
+  int mrow;                    // the member's physical row
+};
+
+template <int CL>
+struct CfShared {
+  static constexpr int NPAR = (CL == 1) ? 1 : 2;  // exchange buffers by step parity
+  ColStat s1[NPAR][CL][kChain];                   // per-CTA column statistics
+  double s2[NPAR][CL][kChain];                    // per-CTA imax-column maxima
+  double V[NPAR][kChain][kChain];                 // V[t][j]: column of member t at member j's row
+  double P2[NPAR][kChain][2];                     // (w_ii, w_ik) of member t
+  Cand cand[kChain];
+  int piv[kNB];  // physical rows of the panel's pivots
+  int scan[kCfWarps];
+};
+
+// Shared-memory layout of one CTA (in doubles), the same in every CTA of the
+// cluster so that a DSMEM address maps to the same array in each: packed
+// own rows of the front (sized for the CTA with the longest share), the
+// panel's W for all physical rows [f][kNBP], the panel's L for own rows
+// [Qmax][kNBP], the chain's columns over own rows [NPAR][2][kChain][Qmax],
+// then perm, ipos, rem and rpos ([f] ints each).
+template <int CL>
+__host__ __device__ __forceinline__ long long cf_layout(int f, long long* oW, long long* oL,
+                                                        long long* oC, long long* oI) {
+  long long t = 0;
+  for (int r = 0; r < CL; r++) {
+    const long long tr = tri_len<CL>(f, r);
+    t = tr > t ? tr : t;
+  }
+  const long long Qmax = (f + CL - 1) / CL;
+  *oW = t;
+  *oL = *oW + (long long)f * kNBP;
+  *oC = *oL + Qmax * kNBP;
+  *oI = *oC + (long long)CfShared<CL>::NPAR * 2 * kChain * Qmax;
+  return *oI + (4LL * f + 1) / 2;
+}
+
+__device__ __forceinline__ void warp_argmax_max(double& bv, int& bi, double& cm) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    keep_larger(bv, bi, ov, oi);
+    cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, o));
+  }
+}
+
+// logical interchange of positions a and b
+__device__ __forceinline__ void perm_swap(int* perm, int* ipos, int a, int b) {
+  if (a == b) return;
+  const int pa = perm[a], pb = perm[b];
+  perm[a] = pb;
+  perm[b] = pa;
+  ipos[pb] = a;
+  ipos[pa] = b;
+}
 
 template <int CL>
 __global__ void __launch_bounds__(kCfThreads)
     cluster_front_kernel(DevPlan p, DevState s, const int* __restrict__ list,
                          const double* __restrict__ vals, const double* __restrict__ diag,
                          FactorParams prm) {
+  constexpr int NPAR = CfShared<CL>::NPAR;
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
   BigFront* B = s.big + list[blockIdx.x / CL];
   extern __shared__ __align__(16) double sm[];
-  // slotA is double-buffered by iteration parity: a CTA may push the next
-  // column partial before a slower CTA has finished reading this one
-  __shared__ CfPart slotA[2][CL], slotB[CL];
-  __shared__ CfRed red;
+  __shared__ CfShared<CL> sh;
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -180,18 +197,31 @@ __global__ void __launch_bounds__(kCfThreads)
   const int nd_in = B->nd_in;
   const int node = B->node;
   const bool root = (B->nc == 0);
+  long long oW, oL, oC, oI;
+  cf_layout<CL>(f, &oW, &oL, &oC, &oI);
+  const int Qmax = (f + CL - 1) / CL;
+  const int Q = (f - rank + CL - 1) / CL;  // own physical rows r = rank + q CL
   double* tri = sm;
-  const long long tl = tri_len<CL>(f, rank);
-  double* col0 = tri + tl;
-  double* col1 = col0 + f;
+  double* Wall = sm + oW;
+  double* Lp = sm + oL;
+  double* colbuf = sm + oC;
+  int* perm = reinterpret_cast<int*>(sm + oI);
+  int* ipos = perm + f;
+  int* rem = ipos + f;
+  int* rpos = rem + f;
   int* fv = s.ivars + B->ioff;
   int* orig = fv + f;
-  // own rows: i = rank + q * CL for q < Q
-  const int Q = (f - rank + CL - 1) / CL;
 
-  // ---- assembly straight into distributed shared memory
-  for (long long t = tid; t < tl; t += kCfThreads) tri[t] = 0.0;
-  cl.sync();
+  // ---- zero the front and the panel arrays, identity order
+  for (long long t = tid; t < oI; t += kCfThreads) sm[t] = 0.0;
+  for (int r = tid; r < f; r += kCfThreads) {
+    perm[r] = r;
+    ipos[r] = r;
+  }
+  csync<CL>(cl);
+
+  // ---- assembly straight into distributed shared memory (physical order is
+  // the front's initial variable order)
   {
     const int64_t e0 = p.scat_ptr[node];
     const int64_t e1 = p.scat_ptr[node + 1];
@@ -202,14 +232,14 @@ __global__ void __launch_bounds__(kCfThreads)
       *dst += vals[p.scat_csr[e]];
     }
   }
-  cl.sync();
+  csync<CL>(cl);
   if (diag) {
     const int v0 = p.var_ptr[node];
     for (int j = gt; j < ns; j += CL * kCfThreads) {
       double* dst = row_ptr<CL>(cl, tri, rank, j) + j;
       *dst += diag[p.node_to_var[v0 + j]];
     }
-    cl.sync();
+    csync<CL>(cl);
   }
   {
     const int kb = p.kid_ptr[node];
@@ -245,278 +275,452 @@ __global__ void __launch_bounds__(kCfThreads)
           *dst += col[r1];
         }
       }
-      cl.sync();
+      csync<CL>(cl);
       off += nd;
     }
   }
 
   // ---- partial factorization of the candidates [0, ncand)
   const double alpha_bk = (1.0 + 4.1231056256176605) / 8.0;  // (1 + sqrt(17)) / 8
+  const bool single = root || prm.cholesky;  // no delays: chains of one
   int k = 0;
   int ncand = fs;
   int npos = 0, nneg = 0;
   double flops = 0.0;
-  int pend = 0, pc = 0;
-  double pd0 = 0.0, pd1 = 0.0, pd2 = 0.0;
+  int stepno = 0;
 
-  int it = 0;
   while (k < ncand) {
-    CfPart* sA = slotA[it & 1];
-    it++;
-    // pivot column k over own rows i > k
-    double bv = -1.0, cmx = 0.0;
-    int bi = INT_MAX;
-    {
-      const int q0 = (k + 1 - rank + CL - 1) / CL > 0 ? (k + 1 - rank + CL - 1) / CL : 0;
-      for (int q = q0 + tid; q < Q; q += kCfThreads) {
-        const int i = rank + q * CL;
-        const double a = fabs(tri[row_off<CL>(i) + k]);
-        if (i < ncand)
-          keep_larger(bv, bi, a, i);
-        else
-          cmx = fmax(cmx, a);
-      }
-    }
-    cf_reduce(red, bv, bi, cmx);
-    {
-      CfPart P;
-      P.v = bv;
-      P.i = bi;
-      P.pad = 0;
-      P.m = cmx;
-      P.x = (k % CL == rank) ? tri[row_off<CL>(k) + k] : 0.0;
-      P.y = 0.0;
-      push<CL>(cl, sA, rank, P);
-    }
-    cl.sync();  // B1
+    const int kstart = k;
+    int kw = 0;
+    while (kw < kNB - 1 && k < ncand) {
+      const int par = (NPAR == 1) ? 0 : (stepno & 1);
+      stepno++;
+      const int nS = single ? 1 : min(kChain, ncand - k);
+      // chain member t sits at logical position k (t = 0) or ncand - t
+      double* cb0 = colbuf + (size_t)(par * 2) * kChain * Qmax;
+      double* cb1 = cb0 + (size_t)kChain * Qmax;
 
-    double gv = -1.0, gm = 0.0;
-    int gi = INT_MAX;
+      // ---- exchange 1: warp t forms the column of chain member t
+      if (warp < nS) {
+        const int t = warp;
+        const int pc = (t == 0) ? perm[k] : perm[ncand - t];
+        double w[kNB];
+        const double* wr = Wall + (size_t)pc * kNBP;
 #pragma unroll
-    for (int r = 0; r < CL; r++) {
-      keep_larger(gv, gi, sA[r].v, sA[r].i);
-      gm = fmax(gm, sA[r].m);
-    }
-    const double wkk = sA[k % CL].x;
-    const bool has = (k + 1 < ncand);
-    const double abswkk = fabs(wkk);
-    const double abswik = has ? gv : 0.0;
-    const int imax = has ? (gi < ncand ? gi : k + 1) : k;
-    const double colmax = fmax(abswik, gm);
-    int step;
-    int kpiv = k;
-    if (prm.cholesky) {
-      step = kOne;
-    } else if (root) {
-      if (fmax(abswkk, colmax) == 0.0)
-        step = kZero;
-      else if (abswkk >= alpha_bk * colmax)
-        step = kOne;
-      else
-        step = kNeedRow;
-    } else if (abswkk >= prm.pivot_tol && abswkk >= prm.ustab * colmax) {
-      step = kOne;
-    } else {
-      step = has ? kNeedRow : kDelay;
-    }
-    double wii = 0.0, wik = 0.0;
-    if (step == kNeedRow) {
-      // column imax below it, and row imax from k to imax (on its owner)
-      double rm = 0.0, dummy = -1.0;
-      int di = INT_MAX;
-      const int q0 = (imax + 1 - rank + CL - 1) / CL > 0 ? (imax + 1 - rank + CL - 1) / CL : 0;
-      for (int q = q0 + tid; q < Q; q += kCfThreads) {
-        const int i = rank + q * CL;
-        rm = fmax(rm, fabs(tri[row_off<CL>(i) + imax]));
-      }
-      const bool own = (imax % CL == rank);
-      if (own) {
-        const double* ri = tri + row_off<CL>(imax);
-        for (int j = k + tid; j < imax; j += kCfThreads) rm = fmax(rm, fabs(ri[j]));
-      }
-      cf_reduce(red, dummy, di, rm);
-      {
-        CfPart P;
-        P.v = 0.0;
-        P.i = 0;
-        P.pad = 0;
-        P.m = rm;
-        P.x = own ? tri[row_off<CL>(imax) + imax] : 0.0;
-        P.y = own ? tri[row_off<CL>(imax) + k] : 0.0;
-        push<CL>(cl, slotB, rank, P);
-      }
-      cl.sync();  // B2
-      double rmax = 0.0;
+        for (int c = 0; c < kNB; c++) w[c] = wr[c];
+        const double* rowc = row_ptr<CL>(cl, tri, rank, pc);
+        double bv = -1.0, cm = 0.0;
+        int bi = INT_MAX;
+        double* out = cb0 + (size_t)t * Qmax;
+        for (int q = lane; q < Q; q += 32) {
+          const int r = rank + q * CL;
+          const int pos = ipos[r];
+          if (pos < k) continue;
+          double v = (r >= pc) ? tri[row_off<CL>(r) + pc] : rowc[r];
+          const double* lr = Lp + (size_t)q * kNBP;
 #pragma unroll
-      for (int r = 0; r < CL; r++) rmax = fmax(rmax, slotB[r].m);
-      wii = slotB[imax % CL].x;
-      wik = slotB[imax % CL].y;
-      const double abswii = fabs(wii);
-      if (root) {
-        if (abswkk >= alpha_bk * colmax * (colmax / rmax)) {
-          step = kOne;
-        } else if (abswii >= alpha_bk * rmax) {
-          step = kOne;
-          kpiv = imax;
-        } else {
-          step = kTwo;
-          kpiv = imax;
+          for (int c = 0; c < kNB; c++) v = fma(-lr[c], w[c], v);
+          out[q] = v;
+          int j = -1;
+          if (pos == k)
+            j = 0;
+          else if (pos > ncand - nS && pos < ncand)
+            j = ncand - pos;
+          if (j >= 0) {
+            for (int d = 0; d < CL; d++) *at_rank<CL>(cl, &sh.V[par][t][j], d, rank) = v;
+          } else if (pos < ncand) {
+            keep_larger(bv, bi, fabs(v), pos);
+          } else {
+            cm = fmax(cm, fabs(v));
+          }
         }
-      } else if (abswii >= prm.pivot_tol && abswii >= prm.ustab * rmax) {
-        step = kOne;
-        kpiv = imax;
+        warp_argmax_max(bv, bi, cm);
+        if (lane < CL) {
+          ColStat st;
+          st.bv = bv;
+          st.cm = cm;
+          st.bi = bi;
+          st.pad = 0;
+          *at_rank<CL>(cl, &sh.s1[par][rank][t], lane, rank) = st;
+        }
+      }
+      csync<CL>(cl);  // B1: statistics and chain entries visible everywhere
+
+      // member t's tests from its column alone, under the hypothesis that
+      // members 0..t-1 were delayed (they are non-candidates by then)
+      if (warp < nS) {
+        const int t = warp;
+        double bv = -1.0, cm = 0.0;
+        int bi = INT_MAX;
+        if (lane < CL) {
+          const ColStat st = sh.s1[par][lane][t];
+          bv = st.bv;
+          cm = st.cm;
+          bi = st.bi;
+        }
+        warp_argmax_max(bv, bi, cm);
+        if (lane == 0) {
+          for (int j = 0; j < nS; j++) {
+            if (j == t) continue;
+            const double a = fabs(sh.V[par][t][j]);
+            if (j > t)
+              keep_larger(bv, bi, a, ncand - j);  // a later member, still a candidate
+            else
+              cm = fmax(cm, a);  // an earlier member, delayed
+          }
+          const int nc_t = ncand - t;
+          const bool has = (k + 1 < nc_t);
+          const double wkk = sh.V[par][t][t];
+          const double abswkk = fabs(wkk);
+          const double abswik = has ? bv : 0.0;
+          const int il = has ? (bi < nc_t ? bi : k + 1) : k;
+          // positions other than k below ncand - t still hold what perm says
+          const int ip = (il == k) ? ((t == 0) ? perm[k] : perm[ncand - t]) : perm[il];
+          const double colmax = fmax(abswik, cm);
+          int d1;
+          if (prm.cholesky) {
+            d1 = kOne;
+          } else if (root) {
+            if (fmax(abswkk, colmax) == 0.0)
+              d1 = kZero;
+            else if (abswkk >= alpha_bk * colmax)
+              d1 = kOne;
+            else
+              d1 = kNeedRow;
+          } else if (abswkk >= prm.pivot_tol && abswkk >= prm.ustab * colmax) {
+            d1 = kOne;
+          } else {
+            d1 = has ? kNeedRow : kDelay;
+          }
+          Cand& c = sh.cand[t];
+          c.wkk = wkk;
+          c.abswik = abswik;
+          c.colmax = colmax;
+          c.dec1 = d1;
+          c.dec2 = kDelay;
+          c.imaxp = ip;
+          c.mrow = (t == 0) ? perm[k] : perm[ncand - t];
+        }
+      }
+      __syncthreads();
+
+      // members that need their imax column: those before the first member
+      // accepted from its column alone
+      unsigned need2 = 0u;
+      for (int t = 0; t < nS; t++) {
+        const int d1 = sh.cand[t].dec1;
+        if (d1 == kOne || d1 == kZero) break;
+        if (d1 == kNeedRow) need2 |= 1u << t;
+      }
+      if (need2) {
+        // ---- exchange 2: warp t forms the imax column of member t
+        if (need2 & (1u << warp)) {
+          const int t = warp;
+          const int pc = sh.cand[t].imaxp;
+          double w[kNB];
+          const double* wr = Wall + (size_t)pc * kNBP;
+#pragma unroll
+          for (int c = 0; c < kNB; c++) w[c] = wr[c];
+          const double* rowc = row_ptr<CL>(cl, tri, rank, pc);
+          double rm = 0.0;
+          double* out = cb1 + (size_t)t * Qmax;
+          const double* colk = cb0 + (size_t)t * Qmax;
+          for (int q = lane; q < Q; q += 32) {
+            const int r = rank + q * CL;
+            if (ipos[r] < k) continue;
+            double v = (r >= pc) ? tri[row_off<CL>(r) + pc] : rowc[r];
+            const double* lr = Lp + (size_t)q * kNBP;
+#pragma unroll
+            for (int c = 0; c < kNB; c++) v = fma(-lr[c], w[c], v);
+            out[q] = v;
+            if (r == pc) {
+              const double wik = colk[q];
+              for (int d = 0; d < CL; d++) {
+                double* dst = at_rank<CL>(cl, &sh.P2[par][t][0], d, rank);
+                dst[0] = v;
+                dst[1] = wik;
+              }
+            } else {
+              rm = fmax(rm, fabs(v));
+            }
+          }
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) rm = fmax(rm, __shfl_xor_sync(0xffffffffu, rm, o));
+          if (lane < CL) *at_rank<CL>(cl, &sh.s2[par][rank][t], lane, rank) = rm;
+        }
+        csync<CL>(cl);  // B2
+        if (need2 & (1u << warp)) {
+          const int t = warp;
+          double rm = (lane < CL) ? sh.s2[par][lane][t] : 0.0;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) rm = fmax(rm, __shfl_xor_sync(0xffffffffu, rm, o));
+          if (lane == 0) {
+            Cand& c = sh.cand[t];
+            const double wii = sh.P2[par][t][0];
+            const double wik = sh.P2[par][t][1];
+            const double abswii = fabs(wii);
+            const double abswkk = fabs(c.wkk);
+            int d2;
+            if (root) {
+              if (abswkk >= alpha_bk * c.colmax * (c.colmax / rm))
+                d2 = kOne;
+              else if (abswii >= alpha_bk * rm)
+                d2 = kOneImax;
+              else
+                d2 = kTwo;
+            } else if (abswii >= prm.pivot_tol && abswii >= prm.ustab * rm) {
+              d2 = kOneImax;
+            } else {
+              const double det = fabs(c.wkk * wii - wik * wik);
+              d2 = kDelay;
+              if (det >= prm.pivot_tol) {
+                const double delta = det / fmax(abswii + c.abswik, abswkk + c.abswik);
+                if (delta >= prm.ustab * c.colmax && delta >= prm.ustab * rm) d2 = kTwo;
+              }
+            }
+            c.rmax = rm;
+            c.wii = wii;
+            c.wik = wik;
+            c.dec2 = d2;
+          }
+        }
+        __syncthreads();
+      }
+
+      // ---- replay the sequential decisions: delays up to the first
+      // accepted member
+      int tacc = nS;
+      int kind = kDelay;
+      for (int t = 0; t < nS; t++) {
+        const int d1 = sh.cand[t].dec1;
+        if (d1 == kOne || d1 == kZero) {
+          tacc = t;
+          kind = d1;
+          break;
+        }
+        if (d1 == kNeedRow && sh.cand[t].dec2 != kDelay) {
+          tacc = t;
+          kind = sh.cand[t].dec2;
+          break;
+        }
+      }
+      const int ndelay = tacc;  // members before tacc (all nS when none accepted)
+      if (tacc == nS) {
+        // member t goes to ncand-1-t: the reference's swap with the last
+        // candidate, ncand shrinking by one each time
+        if (tid == 0)
+          for (int t = 0; t < ndelay; t++) perm_swap(perm, ipos, k, ncand - 1 - t);
+        ncand -= ndelay;
+        __syncthreads();
+        continue;
+      }
+      const Cand& ca = sh.cand[tacc];
+      const int nstep = (kind == kTwo) ? 2 : 1;
+      const int pk = ca.mrow;
+      const int pi = ca.imaxp;
+      // accepted columns: the member's column at k, or the imax column at k
+      // (1x1 at imax); a 2x2 takes both
+      const double* colA = ((kind == kOneImax) ? cb1 : cb0) + (size_t)tacc * Qmax;
+      const double* colB = cb1 + (size_t)tacc * Qmax;
+      const int p0 = (kind == kOneImax) ? pi : pk;
+      // W columns: every CTA gathers the accepted columns from their owners
+      // (entries of eliminated rows are gathered too and never read)
+      for (int r = tid; r < f; r += kCfThreads) {
+        const int o = r % CL;
+        const int qq = r / CL;
+        Wall[(size_t)r * kNBP + kw] = at_rank<CL>(cl, colA, o, rank)[qq];
+        if (nstep == 2) Wall[(size_t)r * kNBP + kw + 1] = at_rank<CL>(cl, colB, o, rank)[qq];
+      }
+      // L columns on own rows; the pivot rows keep D
+      if (nstep == 1) {
+        const double d = (kind == kOneImax) ? ca.wii : ca.wkk;
+        const double dinv = (kind == kZero || (root && d == 0.0)) ? 0.0 : 1.0 / d;
+        for (int q = tid; q < Q; q += kCfThreads) {
+          const int r = rank + q * CL;
+          Lp[(size_t)q * kNBP + kw] = (r == p0) ? d : colA[q] * dinv;
+        }
+        if (tid == 0) {
+          sh.piv[kw] = p0;
+          if (rank == 0) {
+            if (d >= 0.0)
+              npos++;
+            else
+              nneg++;
+            flops += 2.0 * (double)(f - k) * (kw + 1);
+          }
+        }
       } else {
-        const double det = fabs(wkk * wii - wik * wik);
-        step = kDelay;
-        if (det >= prm.pivot_tol) {
-          const double delta = det / fmax(abswii + abswik, abswkk + abswik);
-          if (delta >= prm.ustab * colmax && delta >= prm.ustab * rmax) {
-            step = kTwo;
-            kpiv = imax;
+        const double d11 = ca.wkk, d21 = ca.wik, d22 = ca.wii;
+        const double det = d11 * d22 - d21 * d21;
+        const double detinv = 1.0 / det;
+        const double i00 = d22 * detinv, i01 = -d21 * detinv, i11 = d11 * detinv;
+        for (int q = tid; q < Q; q += kCfThreads) {
+          const int r = rank + q * CL;
+          double* lr = Lp + (size_t)q * kNBP;
+          if (r == pk) {
+            lr[kw] = d11;
+            lr[kw + 1] = 0.0;
+          } else if (r == pi) {
+            lr[kw] = d21;
+            lr[kw + 1] = d22;
+          } else {
+            const double a = colA[q], b = colB[q];
+            lr[kw] = a * i00 + b * i01;
+            lr[kw + 1] = a * i01 + b * i11;
+          }
+        }
+        if (tid == 0) {
+          sh.piv[kw] = pk;
+          sh.piv[kw + 1] = pi;
+          if (rank == 0) {
+            fv[pk] = -(fv[pk] + 1);
+            fv[pi] = -(fv[pi] + 1);
+            if (det >= 0.0) {
+              if (d11 >= 0.0)
+                npos += 2;
+              else
+                nneg += 2;
+            } else {
+              npos++;
+              nneg++;
+            }
+            flops += 4.0 * (double)(f - k) * (kw + 2);
           }
         }
       }
+      // the logical order: the delays, then the pivot interchange (imax to
+      // k for a 1x1 at imax, to k + 1 for a 2x2)
+      if (tid == 0) {
+        for (int t = 0; t < ndelay; t++) perm_swap(perm, ipos, k, ncand - 1 - t);
+        if (kind == kOneImax || kind == kTwo) perm_swap(perm, ipos, k + nstep - 1, ipos[pi]);
+      }
+      ncand -= ndelay;
+      k += nstep;
+      kw += nstep;
+      __syncthreads();  // W, L and the order visible to every warp
     }
 
-    if (step == kDelay) {
-      if (k < ncand - 1) {
-        tri_swap<CL>(cl, tri, rank, f, k, ncand - 1, fv, orig);
-        cl.sync();  // B3
-      }
-      ncand -= 1;
-      continue;
-    }
-    const int nstep = (step == kTwo) ? 2 : 1;
-    const int ksrc = k + nstep - 1;
-    if (kpiv != ksrc) {
-      tri_swap<CL>(cl, tri, rank, f, ksrc, kpiv, fv, orig);
-      cl.sync();  // B3
-    }
-
-    // deferred scaling of the previous pivot column(s) (every CTA gathered
-    // them before the barrier above; swaps since then commute with it)
-    if (pend) {
-      const int from = pc + pend;
-      const int q0 = (from - rank + CL - 1) / CL > 0 ? (from - rank + CL - 1) / CL : 0;
-      for (int q = q0 + tid; q < Q; q += kCfThreads) {
-        double* ri = tri + row_off<CL>(rank + q * CL);
-        if (pend == 1) {
-          ri[pc] *= pd0;
-        } else {
-          const double a = ri[pc], b = ri[pc + 1];
-          ri[pc] = a * pd0 + b * pd1;
-          ri[pc + 1] = a * pd1 + b * pd2;
-        }
-      }
-    }
-    // gather the pivot column(s) below the pivot block from their owners
-    const int k1 = k + nstep;  // first row below the pivot block
-    for (int j = k1 + tid; j < f; j += kCfThreads) {
-      const double* rj = row_ptr<CL>(cl, tri, rank, j);
-      col0[j] = rj[k];
-      if (nstep == 2) col1[j] = rj[k + 1];
-    }
-    __syncthreads();
-    // rank-1 / rank-2 update of own rows i >= k1, columns j in [k1, i]
-    double dinv = 0.0, i00 = 0.0, i01 = 0.0, i11 = 0.0;
-    double d11 = 0.0, d21 = 0.0, d22 = 0.0;
-    if (nstep == 1) {
-      const double d = (kpiv != k) ? wii : wkk;
-      dinv = (step == kZero || (root && d == 0.0)) ? 0.0 : 1.0 / d;
-      if (rank == 0 && tid == 0) {
-        if (d >= 0.0)
-          npos++;
-        else
-          nneg++;
-        const double r = (double)(f - k - 1);
-        flops += r * (r + 1.0) + r;
-      }
-    } else {
-      d11 = wkk;
-      d21 = wik;
-      d22 = wii;
-      const double det = d11 * d22 - d21 * d21;
-      const double detinv = 1.0 / det;
-      i00 = d22 * detinv;
-      i01 = -d21 * detinv;
-      i11 = d11 * detinv;
-      if (rank == 0 && tid == 0) {
-        fv[k] = -(fv[k] + 1);
-        fv[k + 1] = -(fv[k + 1] + 1);
-        if (det >= 0.0) {
-          if (d11 >= 0.0)
-            npos += 2;
+    if (kw > 0) {
+      // the panel's L (and D) into the front's slots: row r, panel column c
+      // (pivot row pc, logical position kstart + c) goes to slot {r, pc};
+      // logical-lower entries only
+      for (int q = warp; q < Q; q += kCfWarps) {
+        const int r = rank + q * CL;
+        const int pos = ipos[r];
+        if (pos < kstart) continue;
+        const double* lr = Lp + (size_t)q * kNBP;
+        const long long ro = row_off<CL>(r);
+        for (int c = lane; c < kw; c += 32) {
+          if (pos < kstart + c) continue;
+          const int pc = sh.piv[c];
+          if (r >= pc)
+            tri[ro + pc] = lr[c];
           else
-            nneg += 2;
-        } else {
-          npos++;
-          nneg++;
-        }
-        const double r = (double)(f - k - 2);
-        flops += 2.0 * r * (r + 1.0) + 6.0 * r;
-      }
-    }
-    {
-      const int q0 = (k1 - rank + CL - 1) / CL > 0 ? (k1 - rank + CL - 1) / CL : 0;
-      for (int q = q0 + warp; q < Q; q += kCfWarps) {
-        const int i = rank + q * CL;
-        double* ri = tri + row_off<CL>(i);
-        if (nstep == 1) {
-          const double li = ri[k] * dinv;
-          for (int j = k1 + lane; j <= i; j += 32) ri[j] = fma(-li, col0[j], ri[j]);
-        } else {
-          const double a = ri[k], b = ri[k + 1];
-          const double l0 = a * i00 + b * i01;
-          const double l1 = a * i01 + b * i11;
-          for (int j = k1 + lane; j <= i; j += 32)
-            ri[j] = fma(-l0, col0[j], fma(-l1, col1[j], ri[j]));
+            row_ptr<CL>(cl, tri, rank, pc)[r] = lr[c];
         }
       }
-    }
-    pend = nstep;
-    pc = k;
-    if (nstep == 1) {
-      pd0 = dinv;
-    } else {
-      pd0 = i00;
-      pd1 = i01;
-      pd2 = i11;
-    }
-    k += nstep;
-    // the next step reads only this CTA's own rows before its barrier
-    __syncthreads();
-  }
-  cl.sync();  // all gathers of the last pivot column are done
-  if (pend) {
-    const int from = pc + pend;
-    const int q0 = (from - rank + CL - 1) / CL > 0 ? (from - rank + CL - 1) / CL : 0;
-    for (int q = q0 + tid; q < Q; q += kCfThreads) {
-      double* ri = tri + row_off<CL>(rank + q * CL);
-      if (pend == 1) {
-        ri[pc] *= pd0;
-      } else {
-        const double a = ri[pc], b = ri[pc + 1];
-        ri[pc] = a * pd0 + b * pd1;
-        ri[pc + 1] = a * pd1 + b * pd2;
+      // remaining physical rows, sorted: rem[0..nrem), rpos[r] = index
+      {
+        const int per = (f + kCfThreads - 1) / kCfThreads;
+        const int a0 = tid * per;
+        const int a1 = min(f, a0 + per);
+        int cnt = 0;
+        for (int r = a0; r < a1; r++) cnt += (ipos[r] >= k);
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        if (lane == 31) sh.scan[warp] = incl;
+        __syncthreads();
+        int base = 0;
+        for (int w2 = 0; w2 < warp; w2++) base += sh.scan[w2];
+        int idx = base + incl - cnt;
+        for (int r = a0; r < a1; r++) {
+          if (ipos[r] >= k) {
+            rem[idx] = r;
+            rpos[r] = idx;
+            idx++;
+          }
+        }
+        __syncthreads();
       }
+      // rank-kw trailing update of own remaining rows over remaining
+      // columns (physical c <= r); two rows per warp pass share the W loads
+      for (int qa = warp; qa < Q; qa += 2 * kCfWarps) {
+        const int qb = qa + kCfWarps;
+        const int ra = rank + qa * CL;
+        const int rb = rank + qb * CL;
+        const bool aon = ipos[ra] >= k;
+        const bool bon = (qb < Q) && ipos[rb] >= k;
+        if (!aon && !bon) continue;
+        const int ja = aon ? rpos[ra] : -1;
+        const int jb = bon ? rpos[rb] : -1;
+        const int jmax = ja > jb ? ja : jb;
+        double la[kNB], lb[kNB];
+        const double* lra = Lp + (size_t)qa * kNBP;
+        const double* lrb = Lp + (size_t)(bon ? qb : qa) * kNBP;
+#pragma unroll
+        for (int c = 0; c < kNB; c++) {
+          la[c] = aon ? lra[c] : 0.0;
+          lb[c] = bon ? lrb[c] : 0.0;
+        }
+        double* ta = tri + row_off<CL>(ra);
+        double* tb = tri + row_off<CL>(bon ? rb : ra);
+        for (int j = lane; j <= jmax; j += 32) {
+          const int c = rem[j];
+          const double* wc = Wall + (size_t)c * kNBP;
+          double acca = 0.0, accb = 0.0;
+#pragma unroll
+          for (int cc = 0; cc < kNB; cc++) {
+            const double wv = wc[cc];
+            acca = fma(la[cc], wv, acca);
+            accb = fma(lb[cc], wv, accb);
+          }
+          if (j <= ja) ta[c] -= acca;
+          if (j <= jb) tb[c] -= accb;
+        }
+      }
+      if (rank == 0 && tid == 0) {
+        const double r = (double)(f - k);
+        flops += r * (r + 1.0) * kw;
+      }
+      __syncthreads();
+      for (int t = tid; t < Q * kNBP; t += kCfThreads) Lp[t] = 0.0;
+      csync<CL>(cl);  // updates and L slots visible before the next panel
     }
   }
-  __syncthreads();
 
   // ---- write the factor columns (f x npiv, ld f) and the contribution
-  // block ((f-npiv)^2, ld f-npiv) into the front's pool region
+  // block ((f-npiv)^2, ld f-npiv) in logical order into the pool region
   const int npiv = k;
   const int m = f - npiv;
   double* Lg = s.dpool + B->doff;
   double* Cg = Lg + (size_t)f * npiv;
-  for (int q = warp; q < Q; q += kCfWarps) {
-    const int i = rank + q * CL;
-    const double* ri = tri + row_off<CL>(i);
-    const int jl = i + 1 < npiv ? i + 1 : npiv;
-    for (int j = lane; j < jl; j += 32) Lg[i + (size_t)f * j] = ri[j];
-    if (i >= npiv) {
-      const int pp = i - npiv;
-      for (int qq = lane; qq <= pp; qq += 32) Cg[pp + (size_t)m * qq] = ri[npiv + qq];
+  for (int j = rank + CL * warp; j < f; j += CL * kCfWarps) {
+    const int pj = perm[j];
+    for (int i = j + lane; i < f; i += 32) {
+      const int pi = perm[i];
+      const int hi = pi >= pj ? pi : pj;
+      const int lo = pi >= pj ? pj : pi;
+      const double v = row_ptr<CL>(cl, tri, rank, hi)[lo];
+      if (j < npiv)
+        Lg[i + (size_t)f * j] = v;
+      else
+        Cg[(i - npiv) + (size_t)m * (j - npiv)] = v;
+    }
+  }
+  if (rank == 0) {
+    // the front's variables in logical order (rem / rpos are free now)
+    for (int i = tid; i < f; i += kCfThreads) {
+      rem[i] = fv[perm[i]];
+      rpos[i] = orig[perm[i]];
+    }
+    __syncthreads();
+    for (int i = tid; i < f; i += kCfThreads) {
+      fv[i] = rem[i];
+      orig[i] = rpos[i];
     }
   }
   if (rank == 0 && tid == 0) {
@@ -526,9 +730,11 @@ __global__ void __launch_bounds__(kCfThreads)
     B->npos += npos;
     B->nneg += nneg;
     B->flops += flops;
+    atomicAdd(s.flops + 4, flops);
     B->pad = 1;  // packed output layout: CB after L with ld m
     B->state = 2;
   }
+  csync<CL>(cl);  // no CTA leaves while others read its shared memory
 }
 
 template <int CL>
@@ -552,15 +758,16 @@ cudaError_t launch_cf(const DevPlan& p, const DevState& s, const int* list, int 
 
 template <int CL>
 size_t cf_smem(int fmax) {
-  long long worst = 0;
-  for (int r = 0; r < CL; r++) {
-    const long long t = tri_len<CL>(fmax, r);
-    if (t > worst) worst = t;
-  }
-  return (size_t)(worst + 2LL * fmax) * sizeof(double);
+  long long oW, oL, oC, oI;
+  return (size_t)cf_layout<CL>(fmax, &oW, &oL, &oC, &oI) * sizeof(double);
 }
 
-constexpr size_t kCfSmemMax = 224 * 1024;
+// dynamic shared memory available next to the kernel's static arrays
+// (227 KB per CTA on sm_100, minus those and a small margin)
+template <int CL>
+constexpr size_t cf_dyn_max() {
+  return 232448 - sizeof(CfShared<CL>) - 1024;
+}
 
 }  // namespace
 
@@ -569,15 +776,15 @@ int cluster_front_limit(int cl_index) {
   static int lim[5] = {0, 0, 0, 0, 0};
   if (lim[0] == 0) {
     int f;
-    for (f = kSmemFrontMax; cf_smem<1>(f + 1) <= kCfSmemMax; f++) {}
+    for (f = kSmemFrontMax; cf_smem<1>(f + 1) <= cf_dyn_max<1>(); f++) {}
     lim[0] = f;
-    for (f = lim[0]; cf_smem<2>(f + 1) <= kCfSmemMax; f++) {}
+    for (f = lim[0]; cf_smem<2>(f + 1) <= cf_dyn_max<2>(); f++) {}
     lim[1] = f;
-    for (f = lim[1]; cf_smem<4>(f + 1) <= kCfSmemMax; f++) {}
+    for (f = lim[1]; cf_smem<4>(f + 1) <= cf_dyn_max<4>(); f++) {}
     lim[2] = f;
-    for (f = lim[2]; cf_smem<8>(f + 1) <= kCfSmemMax; f++) {}
+    for (f = lim[2]; cf_smem<8>(f + 1) <= cf_dyn_max<8>(); f++) {}
     lim[3] = f;
-    for (f = lim[3]; cf_smem<16>(f + 1) <= kCfSmemMax; f++) {}
+    for (f = lim[3]; cf_smem<16>(f + 1) <= cf_dyn_max<16>(); f++) {}
     lim[4] = f;
   }
   return lim[cl_index];
@@ -586,19 +793,19 @@ int cluster_front_limit(int cl_index) {
 cudaError_t configure_cluster_front_kernels() {
   cudaError_t e;
   e = cudaFuncSetAttribute(cluster_front_kernel<1>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCfSmemMax);
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cf_dyn_max<1>());
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(cluster_front_kernel<2>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCfSmemMax);
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cf_dyn_max<2>());
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(cluster_front_kernel<4>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCfSmemMax);
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cf_dyn_max<4>());
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(cluster_front_kernel<8>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCfSmemMax);
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cf_dyn_max<8>());
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(cluster_front_kernel<16>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCfSmemMax);
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cf_dyn_max<16>());
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(cluster_front_kernel<16>,
                               cudaFuncAttributeNonPortableClusterSizeAllowed, 1);

@@ -9,6 +9,9 @@
 
 namespace b200ldl {
 
+// Work counters accumulated on the device per factorization.
+constexpr int kWork = 5;
+
 // Kernel classes timed by the optional profiler.
 enum ProfPhase : int {
   kPhFront = 0,     // per-level front kernels (assembly + factor in shared memory)
@@ -17,7 +20,8 @@ enum ProfPhase : int {
   kPhBigUpd = 3,    // tiled trailing update
   kPhFwd = 4,       // forward solve
   kPhBwd = 5,       // backward solve
-  kPhN = 6
+  kPhCluster = 6,   // fronts factored on chip in a cluster's shared memory
+  kPhN = 7
 };
 
 // CUDA-event timing of kernel classes on the launching stream, plus a count
@@ -131,8 +135,9 @@ struct DevState {
   int64_t* u_off;   // [nn] into the solve's update-vector pool (units of rows)
   int* err;         // [4]: [0] overflow flag, [1] node of first error
   int* inertia;     // [2] pos, neg
-  double* flops;    // [4] executed flops: [0] all fronts, [1] big panels,
-                    // [2] big trailing updates, [3] trailing-update bytes moved
+  double* flops;    // [kWork] executed flops: [0] all fronts, [1] big panels,
+                    // [2] big trailing updates, [3] trailing-update bytes
+                    // moved, [4] fronts factored on chip in a cluster
   BigFront* big;    // [nn] big fronts of the current level
   int* big_meta;    // [16]: count, max f, max fs, count large, max fs large,
                     // class counts [5..9], class max f [10..14]
@@ -194,5 +199,17 @@ int launch_backward_level(const DevPlan& p, const DevState& s,
                           const int* level_nodes, int count, double* x,
                           int ldx, int nrhs, int fmax, cudaStream_t stream);
 cudaError_t configure_solve_kernels();
+
+// residuals and refinement helpers (refine.cu)
+int refine_max_rhs();
+void launch_residual(int n, const int* rowp, const int* cols, const double* vals,
+                     const double* diag, const double* x, int ldx, const double* b, int ldb,
+                     double* r, int ldr, int nr, cudaStream_t st);
+void launch_colmax(int n, const double* v, int ld, int nr, double* out, cudaStream_t st);
+void launch_infnorm(int n, const int* rowp, const int* cols, const double* vals,
+                    const double* diag, double* out, cudaStream_t st);
+void launch_axpy(int n, int nr, const double* d, int ldd, double* x, int ldx, cudaStream_t st);
+void launch_copy_cols(int n, int nr, const double* src, int lds, double* dst, int ldd,
+                      cudaStream_t st);
 
 }  // namespace b200ldl

@@ -233,6 +233,39 @@ class SparseLDL:
             x[:] = a
         return None
 
+    def solve_refine(self, b, max_iter: int = 5, tol: float = 1e-12, diagonal=None):
+        """x = K^-1 b with FP64 iterative refinement against the CSR values
+        (device path: ``b`` a torch CUDA tensor, [n] or [n, k] with the n
+        rows first). Returns (x, berr per column, corrections used)."""
+        import torch
+
+        vals = _values_of(self.mat)
+        diag = _values_of(diagonal)
+        if not (_is_torch(vals) and vals.is_cuda):
+            raise TypeError("solve_refine needs the CSR values on the GPU (torch CUDA tensor)")
+        dev = vals.device
+        bb = b if b.dim() == 2 else b.unsqueeze(1)
+        bcm = bb.t().contiguous().t()  # column-major copy
+        x = torch.empty_like(bcm)
+        x = x.t().contiguous().t()
+        nrhs = bcm.shape[1]
+        d = None
+        if diag is not None:
+            d = diag if _is_torch(diag) else torch.as_tensor(np.asarray(diag), device=dev)
+            d = d.contiguous().to(device=dev, dtype=torch.float64)
+        berr = np.zeros(nrhs)
+        iters = ctypes.c_int()
+        self._sync_stream(vals)
+        st = self._lib.b200ldl_solve_refine(
+            self._h, ctypes.c_void_p(vals.data_ptr()),
+            ctypes.c_void_p(d.data_ptr()) if d is not None else None, nrhs,
+            ctypes.c_void_p(bcm.data_ptr()), bcm.stride(1), ctypes.c_void_p(x.data_ptr()),
+            x.stride(1), int(max_iter), float(tol), berr.ctypes.data_as(_native._f64p),
+            ctypes.byref(iters))
+        _native.check(self._h, st, "solve_refine")
+        out = x if b.dim() == 2 else x[:, 0]
+        return out, berr, iters.value
+
     def get_inertia(self):
         p = ctypes.c_int()
         q = ctypes.c_int()
@@ -276,7 +309,7 @@ class SparseLDL:
 
     # -- profiling ---------------------------------------------------------------
     PHASES = ("fronts", "big_assembly", "big_panel", "big_update", "solve_forward",
-              "solve_backward")
+              "solve_backward", "cluster_fronts")
 
     def set_profiling(self, on: bool):
         self._lib.b200ldl_set_profiling(self._h, 1 if on else 0)
@@ -288,9 +321,10 @@ class SparseLDL:
         return int(self._lib.b200ldl_launch_count(self._h))
 
     def work(self) -> dict:
-        v = np.zeros(4)
-        self._lib.b200ldl_work(self._h, v.ctypes.data_as(_native._f64p), 4)
-        return {"flops": v[0], "panel_flops": v[1], "update_flops": v[2], "update_bytes": v[3]}
+        v = np.zeros(5)
+        self._lib.b200ldl_work(self._h, v.ctypes.data_as(_native._f64p), 5)
+        return {"flops": v[0], "panel_flops": v[1], "update_flops": v[2], "update_bytes": v[3],
+                "cluster_flops": v[4]}
 
     def profile(self) -> list:
         """Per kernel class: device milliseconds (CUDA events), launches, and

@@ -302,8 +302,11 @@ def run_ours(args, world, rank, local):
     peaks = load_peaks()
     algo = {
         # dense partial factorizations outside the big-front path (flops)
-        "fronts": ("tensor", work["flops"] - work["panel_flops"] - work["update_flops"]),
+        "fronts": ("tensor", work["flops"] - work["panel_flops"] - work["update_flops"]
+                   - work["cluster_flops"]),
         "big_panel": ("tensor", work["panel_flops"]),
+        # whole fronts factored in a cluster's distributed shared memory
+        "cluster_fronts": ("tensor", work["cluster_flops"]),
         # rank-kw updates: trailing lower triangle read + written, panels read
         "big_update": ("hbm", work["update_bytes"]),
         # contribution blocks read into the fronts (bytes)

@@ -76,6 +76,22 @@ int b200ldl_solve(b200ldl_t h, int nrhs, double* x, int ldx);
 /* Same with a HOST array x (copied in and out). */
 int b200ldl_solve_host(b200ldl_t h, int nrhs, double* x, int ldx);
 
+/* Solve with FP64 iterative refinement against the matrix itself: x = K^-1 b
+ * by the stored factor, then up to max_iter corrections x += K^-1 (b - K x)
+ * with the residual from the CSR values `vals` and `diag` (DEVICE pointers,
+ * the same matrix that was factored, or its exact FP64 version when the
+ * factor is approximate) until every column's backward error
+ * ||b - Kx||_inf / (||K||_inf ||x||_inf + ||b||_inf) is <= tol. b (ldb) is
+ * left unchanged, x (ldx) receives the solution; both DEVICE. berr_out (HOST,
+ * nrhs entries, may be NULL) receives the final backward errors and
+ * iters_out (HOST, may be NULL) the most corrections any column used. The
+ * reference has no refinement (amigo/algorithm/solvers/linear_solver.py:5-35
+ * has no such method although newton_direction.py:6-8 asks for one). */
+int b200ldl_solve_refine(b200ldl_t h, const double* vals, const double* diag,
+                         int nrhs, const double* b, int ldb, double* x,
+                         int ldx, int max_iter, double tol, double* berr_out,
+                         int* iters_out);
+
 /* Inertia of the last factorization: numbers of positive and negative
  * pivots (zero pivots count as positive, as the reference does). Replaces
  * SparseLDL::get_inertia (include/sparse_ldl.h:205-213). */
@@ -113,8 +129,9 @@ int b200ldl_stats(b200ldl_t h, double* stats, int nstats);
  * when enabled, CUDA events on the handle's stream time each kernel class.
  * b200ldl_profile writes, for each class p in {fronts, big-front assembly,
  * big-front panels, big-front trailing updates, forward solve, backward
- * solve}, out[2p] = accumulated milliseconds and out[2p+1] = kernel
- * launches since the last reset. */
+ * solve, fronts factored on chip in a thread-block cluster}, out[2p] =
+ * accumulated milliseconds and out[2p+1] = kernel launches since the last
+ * reset. */
 int b200ldl_set_profiling(b200ldl_t h, int enable);
 int b200ldl_reset_profile(b200ldl_t h);
 int b200ldl_profile(b200ldl_t h, double* out, int n);
@@ -124,7 +141,8 @@ long long b200ldl_launch_count(b200ldl_t h);
 
 /* Work of the last factorization: out[0] = flops executed in all fronts,
  * out[1] = of which in big-front panels, out[2] = in big-front trailing
- * updates, out[3] = bytes moved by the trailing updates. */
+ * updates, out[3] = bytes moved by the trailing updates, out[4] = flops in
+ * fronts factored on chip in a thread-block cluster. */
 int b200ldl_work(b200ldl_t h, double* out, int n);
 
 /* Allocation-free dense solve (no counterpart in the reference; the
