@@ -252,6 +252,7 @@ void build_plan(b200ldl_t h, const int* rowp, const int* cols) {
     ints += 2.0 * f;
     dbl += f * h->h_ns[k] + (double)h->h_nc[k] * h->h_nc[k];
     if (f > kSmemFrontMax) dbl += f * f + 2.0 * f;
+    if (f > cluster_front_limit(4)) dbl += f * f;  // permutation scratch of the chained panels
   }
   const double g = std::max(1.0, h->delay_growth);
   h->icap = (unsigned long long)(ints * g * 1.5) + (1u << 16);
@@ -389,6 +390,7 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
         info.max_fs = meta[2];
         info.count_large = meta[3];
         info.max_fs_large = meta[4];
+        info.max_f_large = meta[15];
         info.cluster_launches = 0;
         for (int c = 0; c < 5; c++) {
           info.class_count[c] = meta[5 + c];

@@ -725,6 +725,8 @@ cudaError_t configure_big_kernels() {
   e = cudaFuncSetAttribute(big_panel_kernel<16>,
                            cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (e != cudaSuccess) return e;
+  e = configure_big_chain_kernel();
+  if (e != cudaSuccess) return e;
   return configure_cluster_front_kernels();
 }
 
@@ -771,10 +773,14 @@ cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevel
     prof.end(kPhBigAsm, stream, 2 + (diag ? 1 : 0) + maxkids);
   }
   const int upd_grid = 148 * 4;
-  for (int st = 0; st < steps; st++) {
+  const bool chained = big_chain_fits(info.max_f_large);
+  const int nsteps = chained ? (info.max_fs_large + kChainPanel - 2) / (kChainPanel - 1) + 1 : steps;
+  for (int st = 0; st < nsteps; st++) {
     cudaError_t e;
     prof.begin(stream);
-    if (CL == 16)
+    if (chained)
+      e = launch_big_chain_panel(s, prm, info.count_large, info.max_f_large, list5, stream);
+    else if (CL == 16)
       e = launch_panel<16>(s, prm, info.count_large, NB, smem, list5, stream);
     else
       e = launch_panel<8>(s, prm, info.count_large, NB, smem, list5, stream);

@@ -40,6 +40,7 @@
 
 #include <climits>
 
+#include "front_common.cuh"
 #include "ldl_internal.h"
 
 namespace cg = cooperative_groups;
@@ -48,20 +49,13 @@ namespace b200ldl {
 
 namespace {
 
+using namespace chain;
+
 constexpr int kCfThreads = 256;
 constexpr int kCfWarps = kCfThreads / 32;
 constexpr int kNB = 16;           // panel width (pivot columns per trailing update)
 constexpr int kNBP = kNB + 1;     // odd row stride of the panel arrays
-constexpr int kChain = kCfWarps;  // candidates evaluated per step, one per warp
-
-enum : int { kDelay = 0, kOne = 1, kTwo = 2, kNeedRow = 3, kZero = 4, kOneImax = 5 };
-
-__device__ __forceinline__ void keep_larger(double& bv, int& bi, double v, int i) {
-  if (v > bv || (v == bv && i < bi)) {
-    bv = v;
-    bi = i;
-  }
-}
+static_assert(kChain == kCfWarps, "one chain member per warp");
 
 // offset of physical row r inside its owner's packed storage (owner r % CL,
 // local row q = r / CL): q (o + 1) + CL q (q - 1) / 2 with o = r % CL
@@ -102,32 +96,10 @@ __device__ __forceinline__ void csync(cg::cluster_group& cl) {
     cl.sync();
 }
 
-// statistics of one candidate column over one CTA's rows outside the chain
-struct ColStat {
-  double bv;  // largest |.| among candidate rows
-  double cm;  // largest |.| among non-candidate rows
-  int bi;     // logical position of bv (smallest on ties)
-  int pad;
-};
-
-// what one chain member's tests need, reduced over the cluster
-struct Cand {
-  double wkk, abswik, colmax;  // pivot, best candidate entry, column max
-  double rmax, wii, wik;       // imax column: max off-diagonal, diagonal, entry at k
-  int dec1;                    // kOne / kZero / kNeedRow / kDelay from the column alone
-  int dec2;                    // kOne / kOneImax / kTwo / kDelay after the imax column
-  int imaxp;                   // imax: physical row
-  int mrow;                    // the member's physical row
-};
-
 template <int CL>
 struct CfShared {
   static constexpr int NPAR = (CL == 1) ? 1 : 2;  // exchange buffers by step parity
-  ColStat s1[NPAR][CL][kChain];                   // per-CTA column statistics
-  double s2[NPAR][CL][kChain];                    // per-CTA imax-column maxima
-  double V[NPAR][kChain][kChain];                 // V[t][j]: column of member t at member j's row
-  double P2[NPAR][kChain][2];                     // (w_ii, w_ik) of member t
-  Cand cand[kChain];
+  ChainXchg<CL, NPAR> x;
   int piv[kNB];  // physical rows of the panel's pivots
   int scan[kCfWarps];
 };
@@ -154,24 +126,51 @@ __host__ __device__ __forceinline__ long long cf_layout(int f, long long* oW, lo
   return *oI + (4LL * f + 1) / 2;
 }
 
-__device__ __forceinline__ void warp_argmax_max(double& bv, int& bi, double& cm) {
+// Column pc of the current Schur complement on this CTA's rows, for one
+// warp: v(r) = F_sym(r, pc) - Lp(r,:) W(pc,:)^T, two rows per lane pass.
+// Rows already eliminated (logical position < k) are skipped; for the
+// others the value is stored in out[q] and handed to use(q, r, pos, v).
+template <int CL, typename Use>
+__device__ __forceinline__ void member_column(cg::cluster_group& cl, double* tri,
+                                              const double* Lp, const double* Wall,
+                                              const int* ipos, int rank, int Q, int pc, int k,
+                                              int lane, double* out, Use use) {
+  double w[kNB];
+  const double* wr = Wall + (size_t)pc * kNBP;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-    keep_larger(bv, bi, ov, oi);
-    cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, o));
+  for (int c = 0; c < kNB; c++) w[c] = wr[c];
+  const double* rowc = row_ptr<CL>(cl, tri, rank, pc);
+  for (int q0 = lane; q0 < Q; q0 += 64) {
+    const int q1 = q0 + 32;
+    const bool h1 = q1 < Q;
+    const int r0 = rank + q0 * CL;
+    const int r1 = rank + (h1 ? q1 : q0) * CL;
+    const int pos0 = ipos[r0];
+    const int pos1 = h1 ? ipos[r1] : -1;
+    const double f0 = (r0 >= pc) ? tri[row_off<CL>(r0) + pc] : rowc[r0];
+    const double f1 = (r1 >= pc) ? tri[row_off<CL>(r1) + pc] : rowc[r1];
+    const double* l0 = Lp + (size_t)q0 * kNBP;
+    const double* l1 = Lp + (size_t)(h1 ? q1 : q0) * kNBP;
+    double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+#pragma unroll
+    for (int c = 0; c < kNB; c += 2) {
+      a0 = fma(l0[c], w[c], a0);
+      a1 = fma(l0[c + 1], w[c + 1], a1);
+      b0 = fma(l1[c], w[c], b0);
+      b1 = fma(l1[c + 1], w[c + 1], b1);
+    }
+    const double v0 = f0 - (a0 + a1);
+    const double v1 = f1 - (b0 + b1);
+    if (pos0 >= k) {
+      out[q0] = v0;
+      use(q0, r0, pos0, v0);
+    }
+    if (h1 && pos1 >= k) {
+      out[q1] = v1;
+      use(q1, r1, pos1, v1);
+    }
   }
-}
-
-// logical interchange of positions a and b
-__device__ __forceinline__ void perm_swap(int* perm, int* ipos, int a, int b) {
-  if (a == b) return;
-  const int pa = perm[a], pb = perm[b];
-  perm[a] = pb;
-  perm[b] = pa;
-  ipos[pb] = a;
-  ipos[pa] = b;
+  __syncwarp();  // reconverge before the caller's warp reductions
 }
 
 template <int CL>
@@ -261,18 +260,35 @@ __global__ void __launch_bounds__(kCfThreads)
           if (p2 >= ns) p2 += nd_in;
         }
         const double* col = cb + (size_t)cld * r2;
-        for (int r1 = r2 + lane; r1 < m; r1 += 32) {
-          int p1;
-          if (r1 < nd) {
-            p1 = off + r1;
-          } else {
-            p1 = cm[r1 - nd];
-            if (p1 >= ns) p1 += nd_in;
+        // four entries per lane pass: their loads are issued before the
+        // read-modify-writes into the front
+        for (int rb = r2 + lane; rb < m; rb += 128) {
+          int p1[4];
+          double v[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const int r1 = rb + 32 * u;
+            p1[u] = -1;
+            if (r1 < m) {
+              int pp;
+              if (r1 < nd) {
+                pp = off + r1;
+              } else {
+                pp = cm[r1 - nd];
+                if (pp >= ns) pp += nd_in;
+              }
+              p1[u] = pp;
+              v[u] = col[r1];
+            }
           }
-          const int hi = p1 >= p2 ? p1 : p2;
-          const int lo = p1 >= p2 ? p2 : p1;
-          double* dst = row_ptr<CL>(cl, tri, rank, hi) + lo;
-          *dst += col[r1];
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            if (p1[u] < 0) continue;
+            const int hi = p1[u] >= p2 ? p1[u] : p2;
+            const int lo = p1[u] >= p2 ? p2 : p1[u];
+            double* dst = row_ptr<CL>(cl, tri, rank, hi) + lo;
+            *dst += v[u];
+          }
         }
       }
       csync<CL>(cl);
@@ -281,7 +297,6 @@ __global__ void __launch_bounds__(kCfThreads)
   }
 
   // ---- partial factorization of the candidates [0, ncand)
-  const double alpha_bk = (1.0 + 4.1231056256176605) / 8.0;  // (1 + sqrt(17)) / 8
   const bool single = root || prm.cholesky;  // no delays: chains of one
   int k = 0;
   int ncand = fs;
@@ -304,36 +319,25 @@ __global__ void __launch_bounds__(kCfThreads)
       if (warp < nS) {
         const int t = warp;
         const int pc = (t == 0) ? perm[k] : perm[ncand - t];
-        double w[kNB];
-        const double* wr = Wall + (size_t)pc * kNBP;
-#pragma unroll
-        for (int c = 0; c < kNB; c++) w[c] = wr[c];
-        const double* rowc = row_ptr<CL>(cl, tri, rank, pc);
         double bv = -1.0, cm = 0.0;
         int bi = INT_MAX;
         double* out = cb0 + (size_t)t * Qmax;
-        for (int q = lane; q < Q; q += 32) {
-          const int r = rank + q * CL;
-          const int pos = ipos[r];
-          if (pos < k) continue;
-          double v = (r >= pc) ? tri[row_off<CL>(r) + pc] : rowc[r];
-          const double* lr = Lp + (size_t)q * kNBP;
-#pragma unroll
-          for (int c = 0; c < kNB; c++) v = fma(-lr[c], w[c], v);
-          out[q] = v;
-          int j = -1;
-          if (pos == k)
-            j = 0;
-          else if (pos > ncand - nS && pos < ncand)
-            j = ncand - pos;
-          if (j >= 0) {
-            for (int d = 0; d < CL; d++) *at_rank<CL>(cl, &sh.V[par][t][j], d, rank) = v;
-          } else if (pos < ncand) {
-            keep_larger(bv, bi, fabs(v), pos);
-          } else {
-            cm = fmax(cm, fabs(v));
-          }
-        }
+        member_column<CL>(cl, tri, Lp, Wall, ipos, rank, Q, pc, k, lane, out,
+                          [&](int q, int r, int pos, double v) {
+                            int j = -1;
+                            if (pos == k)
+                              j = 0;
+                            else if (pos > ncand - nS && pos < ncand)
+                              j = ncand - pos;
+                            if (j >= 0) {
+                              for (int d = 0; d < CL; d++)
+                                *at_rank<CL>(cl, &sh.x.V[par][t][j], d, rank) = v;
+                            } else if (pos < ncand) {
+                              keep_larger(bv, bi, fabs(v), pos);
+                            } else {
+                              cm = fmax(cm, fabs(v));
+                            }
+                          });
         warp_argmax_max(bv, bi, cm);
         if (lane < CL) {
           ColStat st;
@@ -341,183 +345,65 @@ __global__ void __launch_bounds__(kCfThreads)
           st.cm = cm;
           st.bi = bi;
           st.pad = 0;
-          *at_rank<CL>(cl, &sh.s1[par][rank][t], lane, rank) = st;
+          *at_rank<CL>(cl, &sh.x.s1[par][rank][t], lane, rank) = st;
         }
       }
       csync<CL>(cl);  // B1: statistics and chain entries visible everywhere
 
-      // member t's tests from its column alone, under the hypothesis that
-      // members 0..t-1 were delayed (they are non-candidates by then)
-      if (warp < nS) {
-        const int t = warp;
-        double bv = -1.0, cm = 0.0;
-        int bi = INT_MAX;
-        if (lane < CL) {
-          const ColStat st = sh.s1[par][lane][t];
-          bv = st.bv;
-          cm = st.cm;
-          bi = st.bi;
-        }
-        warp_argmax_max(bv, bi, cm);
-        if (lane == 0) {
-          for (int j = 0; j < nS; j++) {
-            if (j == t) continue;
-            const double a = fabs(sh.V[par][t][j]);
-            if (j > t)
-              keep_larger(bv, bi, a, ncand - j);  // a later member, still a candidate
-            else
-              cm = fmax(cm, a);  // an earlier member, delayed
-          }
-          const int nc_t = ncand - t;
-          const bool has = (k + 1 < nc_t);
-          const double wkk = sh.V[par][t][t];
-          const double abswkk = fabs(wkk);
-          const double abswik = has ? bv : 0.0;
-          const int il = has ? (bi < nc_t ? bi : k + 1) : k;
-          // positions other than k below ncand - t still hold what perm says
-          const int ip = (il == k) ? ((t == 0) ? perm[k] : perm[ncand - t]) : perm[il];
-          const double colmax = fmax(abswik, cm);
-          int d1;
-          if (prm.cholesky) {
-            d1 = kOne;
-          } else if (root) {
-            if (fmax(abswkk, colmax) == 0.0)
-              d1 = kZero;
-            else if (abswkk >= alpha_bk * colmax)
-              d1 = kOne;
-            else
-              d1 = kNeedRow;
-          } else if (abswkk >= prm.pivot_tol && abswkk >= prm.ustab * colmax) {
-            d1 = kOne;
-          } else {
-            d1 = has ? kNeedRow : kDelay;
-          }
-          Cand& c = sh.cand[t];
-          c.wkk = wkk;
-          c.abswik = abswik;
-          c.colmax = colmax;
-          c.dec1 = d1;
-          c.dec2 = kDelay;
-          c.imaxp = ip;
-          c.mrow = (t == 0) ? perm[k] : perm[ncand - t];
-        }
-      }
+      // member tests from the columns alone
+      if (warp < nS)
+        decide_column<CL, NPAR>(sh.x, par, warp, lane, nS, k, ncand, root, prm, perm);
       __syncthreads();
 
-      // members that need their imax column: those before the first member
-      // accepted from its column alone
-      unsigned need2 = 0u;
-      for (int t = 0; t < nS; t++) {
-        const int d1 = sh.cand[t].dec1;
-        if (d1 == kOne || d1 == kZero) break;
-        if (d1 == kNeedRow) need2 |= 1u << t;
-      }
+      unsigned acc1;
+      int d1l;
+      const unsigned need2 = need_rows(sh.x.cand, nS, lane, acc1, d1l);
       if (need2) {
         // ---- exchange 2: warp t forms the imax column of member t
         if (need2 & (1u << warp)) {
           const int t = warp;
-          const int pc = sh.cand[t].imaxp;
-          double w[kNB];
-          const double* wr = Wall + (size_t)pc * kNBP;
-#pragma unroll
-          for (int c = 0; c < kNB; c++) w[c] = wr[c];
-          const double* rowc = row_ptr<CL>(cl, tri, rank, pc);
+          const int pc = sh.x.cand[t].imaxp;
           double rm = 0.0;
           double* out = cb1 + (size_t)t * Qmax;
           const double* colk = cb0 + (size_t)t * Qmax;
-          for (int q = lane; q < Q; q += 32) {
-            const int r = rank + q * CL;
-            if (ipos[r] < k) continue;
-            double v = (r >= pc) ? tri[row_off<CL>(r) + pc] : rowc[r];
-            const double* lr = Lp + (size_t)q * kNBP;
-#pragma unroll
-            for (int c = 0; c < kNB; c++) v = fma(-lr[c], w[c], v);
-            out[q] = v;
-            if (r == pc) {
-              const double wik = colk[q];
-              for (int d = 0; d < CL; d++) {
-                double* dst = at_rank<CL>(cl, &sh.P2[par][t][0], d, rank);
-                dst[0] = v;
-                dst[1] = wik;
-              }
-            } else {
-              rm = fmax(rm, fabs(v));
-            }
-          }
+          member_column<CL>(cl, tri, Lp, Wall, ipos, rank, Q, pc, k, lane, out,
+                            [&](int q, int r, int pos, double v) {
+                              if (r == pc) {
+                                const double wik = colk[q];
+                                for (int d = 0; d < CL; d++) {
+                                  double* dst = at_rank<CL>(cl, &sh.x.P2[par][t][0], d, rank);
+                                  dst[0] = v;
+                                  dst[1] = wik;
+                                }
+                              } else {
+                                rm = fmax(rm, fabs(v));
+                              }
+                            });
 #pragma unroll
           for (int o = 16; o > 0; o >>= 1) rm = fmax(rm, __shfl_xor_sync(0xffffffffu, rm, o));
-          if (lane < CL) *at_rank<CL>(cl, &sh.s2[par][rank][t], lane, rank) = rm;
+          if (lane < CL) *at_rank<CL>(cl, &sh.x.s2[par][rank][t], lane, rank) = rm;
         }
         csync<CL>(cl);  // B2
-        if (need2 & (1u << warp)) {
-          const int t = warp;
-          double rm = (lane < CL) ? sh.s2[par][lane][t] : 0.0;
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) rm = fmax(rm, __shfl_xor_sync(0xffffffffu, rm, o));
-          if (lane == 0) {
-            Cand& c = sh.cand[t];
-            const double wii = sh.P2[par][t][0];
-            const double wik = sh.P2[par][t][1];
-            const double abswii = fabs(wii);
-            const double abswkk = fabs(c.wkk);
-            int d2;
-            if (root) {
-              if (abswkk >= alpha_bk * c.colmax * (c.colmax / rm))
-                d2 = kOne;
-              else if (abswii >= alpha_bk * rm)
-                d2 = kOneImax;
-              else
-                d2 = kTwo;
-            } else if (abswii >= prm.pivot_tol && abswii >= prm.ustab * rm) {
-              d2 = kOneImax;
-            } else {
-              const double det = fabs(c.wkk * wii - wik * wik);
-              d2 = kDelay;
-              if (det >= prm.pivot_tol) {
-                const double delta = det / fmax(abswii + c.abswik, abswkk + c.abswik);
-                if (delta >= prm.ustab * c.colmax && delta >= prm.ustab * rm) d2 = kTwo;
-              }
-            }
-            c.rmax = rm;
-            c.wii = wii;
-            c.wik = wik;
-            c.dec2 = d2;
-          }
-        }
+        if (need2 & (1u << warp)) decide_row<CL, NPAR>(sh.x, par, warp, lane, root, prm);
         __syncthreads();
       }
 
       // ---- replay the sequential decisions: delays up to the first
-      // accepted member
-      int tacc = nS;
-      int kind = kDelay;
-      for (int t = 0; t < nS; t++) {
-        const int d1 = sh.cand[t].dec1;
-        if (d1 == kOne || d1 == kZero) {
-          tacc = t;
-          kind = d1;
-          break;
-        }
-        if (d1 == kNeedRow && sh.cand[t].dec2 != kDelay) {
-          tacc = t;
-          kind = sh.cand[t].dec2;
-          break;
-        }
-      }
+      // accepted member; the logical order by warp 0
+      int tacc, kind;
+      replay(sh.x.cand, nS, lane, acc1, d1l, tacc, kind);
       const int ndelay = tacc;  // members before tacc (all nS when none accepted)
+      const int nstep = (kind == kTwo) ? 2 : 1;
+      const int pi_acc = (tacc < nS) ? sh.x.cand[tacc].imaxp : -1;
+      if (warp == 0) reorder(sh.x.cand, perm, ipos, lane, nS, ndelay, k, ncand, kind, nstep, pi_acc);
       if (tacc == nS) {
-        // member t goes to ncand-1-t: the reference's swap with the last
-        // candidate, ncand shrinking by one each time
-        if (tid == 0)
-          for (int t = 0; t < ndelay; t++) perm_swap(perm, ipos, k, ncand - 1 - t);
         ncand -= ndelay;
         __syncthreads();
         continue;
       }
-      const Cand& ca = sh.cand[tacc];
-      const int nstep = (kind == kTwo) ? 2 : 1;
+      const Cand& ca = sh.x.cand[tacc];
       const int pk = ca.mrow;
-      const int pi = ca.imaxp;
+      const int pi = pi_acc;
       // accepted columns: the member's column at k, or the imax column at k
       // (1x1 at imax); a 2x2 takes both
       const double* colA = ((kind == kOneImax) ? cb1 : cb0) + (size_t)tacc * Qmax;
@@ -525,11 +411,24 @@ __global__ void __launch_bounds__(kCfThreads)
       const int p0 = (kind == kOneImax) ? pi : pk;
       // W columns: every CTA gathers the accepted columns from their owners
       // (entries of eliminated rows are gathered too and never read)
-      for (int r = tid; r < f; r += kCfThreads) {
-        const int o = r % CL;
-        const int qq = r / CL;
-        Wall[(size_t)r * kNBP + kw] = at_rank<CL>(cl, colA, o, rank)[qq];
-        if (nstep == 2) Wall[(size_t)r * kNBP + kw + 1] = at_rank<CL>(cl, colB, o, rank)[qq];
+      for (int r0 = tid; r0 < f; r0 += 4 * kCfThreads) {
+        double a[4], b[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int r = r0 + u * kCfThreads;
+          if (r < f) {
+            a[u] = at_rank<CL>(cl, colA, r % CL, rank)[r / CL];
+            if (nstep == 2) b[u] = at_rank<CL>(cl, colB, r % CL, rank)[r / CL];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int r = r0 + u * kCfThreads;
+          if (r < f) {
+            Wall[(size_t)r * kNBP + kw] = a[u];
+            if (nstep == 2) Wall[(size_t)r * kNBP + kw + 1] = b[u];
+          }
+        }
       }
       // L columns on own rows; the pivot rows keep D
       if (nstep == 1) {
@@ -587,12 +486,6 @@ __global__ void __launch_bounds__(kCfThreads)
             flops += 4.0 * (double)(f - k) * (kw + 2);
           }
         }
-      }
-      // the logical order: the delays, then the pivot interchange (imax to
-      // k for a 1x1 at imax, to k + 1 for a 2x2)
-      if (tid == 0) {
-        for (int t = 0; t < ndelay; t++) perm_swap(perm, ipos, k, ncand - 1 - t);
-        if (kind == kOneImax || kind == kTwo) perm_swap(perm, ipos, k + nstep - 1, ipos[pi]);
       }
       ncand -= ndelay;
       k += nstep;

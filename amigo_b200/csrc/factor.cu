@@ -152,8 +152,10 @@ __global__ void __launch_bounds__(kFactorThreads)
     if (io + 2ull * f > s.icap) fail = 1;
     sh_ioff = (long long)io;
     if (big) {
-      // the front itself plus the panel's W columns
-      const unsigned long long need = (unsigned long long)f * f + (unsigned long long)kBigPanelMax * f;
+      // the front itself plus the panel's W columns; fronts above the
+      // on-chip limit also get the chained panel's permutation scratch
+      unsigned long long need = (unsigned long long)f * f + (unsigned long long)kBigPanelMax * f;
+      if (f > s.cf_limit[4]) need += (unsigned long long)(fs + 1) * f;
       const unsigned long long dofs = atomicAdd(s.used + 1, need);
       if (dofs + need > s.dcap) fail = 1;
       sh_doff = (long long)dofs;
@@ -194,6 +196,7 @@ __global__ void __launch_bounds__(kFactorThreads)
       if (cls == 5) {
         const int q = atomicAdd(s.big_meta + 3, 1);
         atomicMax(s.big_meta + 4, fs);
+        atomicMax(s.big_meta + 15, f);
         s.class_list[(size_t)5 * p.num_nodes + q] = slot;
       } else {
         const int q = atomicAdd(s.big_meta + 5 + cls, 1);

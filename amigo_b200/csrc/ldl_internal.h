@@ -116,6 +116,7 @@ struct BigFront {
 };
 
 constexpr int kBigPanelMax = 32;
+constexpr int kChainPanel = 16;  // panel width of the chained big-front kernel
 
 // Mutable state of one factorization (device memory).
 struct DevState {
@@ -170,6 +171,7 @@ struct BigLevelInfo {
   int count_large, max_fs_large;
   int class_count[5], class_maxf[5];
   int cluster_launches;
+  int max_f_large;  // largest front of class 5
 };
 
 // Fronts above kSmemFrontMax are factored on chip by a cluster of 1, 2, 4,
@@ -181,6 +183,13 @@ cudaError_t configure_cluster_front_kernels();
 cudaError_t launch_cluster_fronts(const DevPlan& p, const DevState& s, const int* counts,
                                   const int* maxf, const double* vals, const double* diag,
                                   const FactorParams& prm, cudaStream_t stream, int nn);
+// Class-5 fronts whose panel state fits one cluster's shared memory use the
+// chained panel kernel (big_chain.cu); larger ones the single-candidate one.
+bool big_chain_fits(int f);
+cudaError_t configure_big_chain_kernel();
+cudaError_t launch_big_chain_panel(const DevState& s, const FactorParams& prm, int count,
+                                   int max_f, const int* list, cudaStream_t stream);
+
 cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
                              int maxkids, const FactorParams& prm, const double* vals,
                              const double* diag, cudaStream_t stream, Prof& prof);
