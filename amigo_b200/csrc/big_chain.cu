@@ -62,18 +62,20 @@ __device__ __forceinline__ double fsym(const double* F, int f, int a, int b) {
 }
 
 // Column pc of the panel's Schur complement on this CTA's rows, by one
-// warp; w holds W(pc, :) (zero beyond the panel's width). Four rows per
-// lane pass so that their HBM loads are in flight together.
+// warp; w holds W(pc, :) (zero beyond the panel's width). kRowsPerLane rows
+// per lane pass so that their HBM loads are in flight together (more rows
+// in flight measured slower: the strided loads of the row part queue up).
+constexpr int kRowsPerLane = 4;
 template <typename Use>
 __device__ __forceinline__ void big_member_column(const double* F, int f, const double* Lp,
                                                   const unsigned short* ipos, int r0, int Q,
                                                   int pc, int k, int lane, const double* w,
                                                   double* out, Use use) {
-  for (int qb = lane; qb < Q; qb += 128) {
-    double fv4[4];
-    int pos4[4];
+  for (int qb = lane; qb < Q; qb += 32 * kRowsPerLane) {
+    double fv4[kRowsPerLane];
+    int pos4[kRowsPerLane];
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
+    for (int u = 0; u < kRowsPerLane; u++) {
       const int q = qb + 32 * u;
       pos4[u] = -1;
       fv4[u] = 0.0;
@@ -84,7 +86,7 @@ __device__ __forceinline__ void big_member_column(const double* F, int f, const 
       }
     }
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
+    for (int u = 0; u < kRowsPerLane; u++) {
       if (pos4[u] < k) continue;
       const int q = qb + 32 * u;
       const double* lr = Lp + (size_t)q * kNBP;
@@ -177,7 +179,7 @@ __global__ void __launch_bounds__(kBcThreads)
       double w[kNB];
 #pragma unroll
       for (int c = 0; c < kNB; c++) w[c] = __shfl_sync(0xffffffffu, wl, c);
-      double bv = -1.0, cm = 0.0;
+      double bv = 0.0, cm = 0.0;
       int bi = INT_MAX;
       double* out = cb0 + (size_t)t * R;
       big_member_column(F, f, Lp, ipos, r0, Q, pc, k, lane, w, out,
@@ -240,8 +242,7 @@ __global__ void __launch_bounds__(kBcThreads)
                               rm = fmax(rm, fabs(v));
                             }
                           });
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) rm = fmax(rm, __shfl_xor_sync(0xffffffffu, rm, o));
+        rm = warp_max_nonneg(rm);
         if (lane < kBcCL) *at_rank(cl, &sh.x.s2[par][rank][t], lane, rank) = rm;
       }
       cl.sync();  // B2
@@ -389,13 +390,11 @@ __global__ void __launch_bounds__(kBcThreads)
 
   // ---- the panel's L (and D) into its logical columns; W in logical order
   // for the trailing update
-  for (int q = warp; q < Q; q += kBcWarps) {
-    const int r = r0 + q;
-    const int pos = ipos[r];
-    if (pos < kstart) continue;
-    const double* lr = Lp + (size_t)q * kNBP;
-    for (int c = lane; c < kw; c += 32) {
-      if (pos >= kstart + c) F[pos + (size_t)f * (kstart + c)] = lr[c];
+  for (int c = 0; c < kw; c++) {
+    for (int q = tid; q < Q; q += kBcThreads) {
+      const int r = r0 + q;
+      const int pos = ipos[r];
+      if (pos >= kstart + c) F[pos + (size_t)f * (kstart + c)] = Lp[(size_t)q * kNBP + c];
       if (pos >= k) Wg[(size_t)c * f + pos] = Wph[(size_t)c * f + r];
     }
   }

@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(kCfThreads)
       if (warp < nS) {
         const int t = warp;
         const int pc = (t == 0) ? perm[k] : perm[ncand - t];
-        double bv = -1.0, cm = 0.0;
+        double bv = 0.0, cm = 0.0;
         int bi = INT_MAX;
         double* out = cb0 + (size_t)t * Qmax;
         member_column<CL>(cl, tri, Lp, Wall, ipos, rank, Q, pc, k, lane, out,
@@ -379,8 +379,7 @@ __global__ void __launch_bounds__(kCfThreads)
                                 rm = fmax(rm, fabs(v));
                               }
                             });
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) rm = fmax(rm, __shfl_xor_sync(0xffffffffu, rm, o));
+          rm = warp_max_nonneg(rm);
           if (lane < CL) *at_rank<CL>(cl, &sh.x.s2[par][rank][t], lane, rank) = rm;
         }
         csync<CL>(cl);  // B2

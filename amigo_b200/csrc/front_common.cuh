@@ -28,9 +28,9 @@ __device__ __forceinline__ void keep_larger(double& bv, int& bi, double v, int i
 
 // statistics of one candidate column over one CTA's rows outside the chain
 struct ColStat {
-  double bv;  // largest |.| among candidate rows
+  double bv;  // largest |.| among candidate rows (0 when there is none)
   double cm;  // largest |.| among non-candidate rows
-  int bi;     // logical position of bv (smallest on ties)
+  int bi;     // logical position of bv (smallest on ties; INT_MAX if none)
   int pad;
 };
 
@@ -44,18 +44,30 @@ struct Cand {
   int mrow;                    // the member's physical row
 };
 
-// warp-wide (argmax with the smallest index on ties, max) in every lane:
-// the maxima by butterfly, then the smallest index among the lanes that
-// hold the maximum by an integer min-reduction
+// Warp-wide maximum of a non-negative double in every lane. Non-negative
+// IEEE doubles order like their bit patterns, so the maximum is taken with
+// two 32-bit integer reductions (high word, then low word among the lanes
+// holding the highest high word): exact, and far fewer dependent steps than
+// a butterfly of FP64 compares.
+__device__ __forceinline__ double warp_max_nonneg(double v) {
+  const unsigned long long u = (unsigned long long)__double_as_longlong(v);
+  const unsigned hi = (unsigned)(u >> 32);
+  const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? (unsigned)u : 0u);
+  return __longlong_as_double((long long)(((unsigned long long)mh << 32) | ml));
+}
+
+// warp-wide (argmax with the smallest index on ties, max) of non-negative
+// values in every lane; lanes without a candidate hold (0, INT_MAX)
 __device__ __forceinline__ void warp_argmax_max(double& bv, int& bi, double& cm) {
-  double m = bv;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    cm = fmax(cm, __shfl_xor_sync(0xffffffffu, cm, o));
-  }
-  bi = __reduce_min_sync(0xffffffffu, (bv == m) ? bi : INT_MAX);
-  bv = m;
+  const unsigned long long u = (unsigned long long)__double_as_longlong(bv);
+  const unsigned hi = (unsigned)(u >> 32);
+  const unsigned lo = (unsigned)u;
+  const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+  bi = __reduce_min_sync(0xffffffffu, (hi == mh && lo == ml) ? bi : INT_MAX);
+  bv = __longlong_as_double((long long)(((unsigned long long)mh << 32) | ml));
+  cm = warp_max_nonneg(cm);
 }
 
 constexpr int kChain = 8;  // chain members per step, one per warp
@@ -83,7 +95,7 @@ template <int CL, int NPAR, typename IdxT>
 __device__ __forceinline__ void decide_column(ChainXchg<CL, NPAR>& x, int par, int t, int lane,
                                               int nS, int k, int ncand, bool root,
                                               const FactorParams& prm, const IdxT* perm) {
-  double bv = -1.0, cm = 0.0;
+  double bv = 0.0, cm = 0.0;
   int bi = INT_MAX;
   if (lane < CL) {
     const ColStat st = x.s1[par][lane][t];
@@ -153,8 +165,7 @@ __device__ __forceinline__ void decide_row(ChainXchg<CL, NPAR>& x, int par, int 
                                            bool root, const FactorParams& prm) {
   double rm = (lane < CL) ? x.s2[par][lane][t] : 0.0;
   __syncwarp();
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) rm = fmax(rm, __shfl_xor_sync(0xffffffffu, rm, o));
+  rm = warp_max_nonneg(rm);
   const Cand& c = x.cand[t];
   const double wii = x.P2[par][t][0];
   const double wik = x.P2[par][t][1];
