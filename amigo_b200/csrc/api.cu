@@ -103,7 +103,6 @@ struct b200ldl_handle {
   DevBuf<BigFront> d_big;
   DevBuf<int> d_big_meta;
   DevBuf<int> d_class_list;
-  DevBuf<long long> d_tile_ptr;
   unsigned long long icap = 0, dcap = 0;
   DevState st{};
 
@@ -315,7 +314,6 @@ void upload_plan(b200ldl_t h) {
   CK(h->d_big.alloc(nn));
   CK(h->d_big_meta.alloc(16));
   CK(h->d_class_list.alloc((size_t)6 * std::max(1, nn)));
-  CK(h->d_tile_ptr.alloc(nn + 1));
   h->uploaded = true;
 }
 
@@ -343,7 +341,6 @@ void bind_state(b200ldl_t h) {
   st.big_meta = h->d_big_meta.ptr;
   st.class_list = h->d_class_list.ptr;
   for (int c = 0; c < 5; c++) st.cf_limit[c] = cluster_front_limit(c);
-  st.tile_ptr = h->d_tile_ptr.ptr;
 }
 
 void ensure_pools(b200ldl_t h) {
@@ -367,6 +364,7 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
     CK(cudaMemsetAsync(h->d_used.ptr, 0, 3 * sizeof(unsigned long long), h->stream));
     CK(cudaMemsetAsync(h->d_err.ptr, 0, sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_err.ptr + 1, 0xff, sizeof(int), h->stream));
+    CK(cudaMemsetAsync(h->d_err.ptr + 2, 0, 2 * sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_inertia.ptr, 0, 2 * sizeof(int), h->stream));
     CK(cudaMemsetAsync(h->d_flops.ptr, 0, kWork * sizeof(double), h->stream));
     CK(cudaMemsetAsync(h->d_ndel.ptr, 0, sizeof(int) * std::max(1, h->sym.num_nodes), h->stream));

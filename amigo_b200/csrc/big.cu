@@ -34,6 +34,7 @@ constexpr int kPanelThreads = 256;
 constexpr int kPWarps = kPanelThreads / 32;
 constexpr int kTile = 64;
 constexpr int kUpdThreads = 256;
+constexpr int kUpdMaxFronts = 1024;  // class-5 fronts per level handled by one update launch
 
 __device__ __forceinline__ void keep_larger(double& bv, int& bi, double v, int i) {
   if (v > bv || (v == bv && i < bi)) {
@@ -541,59 +542,74 @@ __global__ void __launch_bounds__(kPanelThreads)
 
 // --------------------------------------------------------- trailing update
 
-__global__ void big_tiles_kernel(DevState s, int nbig) {
-  // one CTA: prefix sum of lower-triangular 64x64 tile counts
-  __shared__ long long carry;
-  if (threadIdx.x == 0) {
-    carry = 0;
-    s.tile_ptr[0] = 0;
-  }
-  __syncthreads();
-  for (int base = 0; base < nbig; base += blockDim.x) {
-    const int i = base + threadIdx.x;
-    long long cnt = 0;
-    if (i < nbig) {
-      const BigFront& B = s.big[i];
-      if (B.state != 2 && B.kw > 0) {
-        const long long t = (B.f - B.k + kTile - 1) / kTile;
-        cnt = t * (t + 1) / 2;
-      }
-    }
-    // inclusive scan in the block (simple, nbig is small)
-    __shared__ long long buf[1024];
-    buf[threadIdx.x] = cnt;
-    __syncthreads();
-    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-      long long v = (threadIdx.x >= (unsigned)o) ? buf[threadIdx.x - o] : 0;
-      __syncthreads();
-      buf[threadIdx.x] += v;
-      __syncthreads();
-    }
-    if (i < nbig) s.tile_ptr[i + 1] = carry + buf[threadIdx.x];
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) carry += buf[threadIdx.x];
-    __syncthreads();
-  }
-}
-
-__global__ void __launch_bounds__(kUpdThreads) big_update_kernel(DevState s, int nbig) {
+// One launch per panel for all class-5 fronts of the level (list5, nl of
+// them): lower-triangular 64x64 tiles of each front's trailing matrix in one
+// tile space; every CTA forms the prefix of tile counts itself. The last CTA
+// to finish closes the panel (work counters, kw = 0, finished fronts done).
+__global__ void __launch_bounds__(kUpdThreads)
+    big_update_kernel(DevState s, const int* __restrict__ list5, int nl) {
   __shared__ double As[kBigPanelMax][kTile];
   __shared__ double Bs[kBigPanelMax][kTile];
-  const long long total = s.tile_ptr[nbig];
-  const int tx = threadIdx.x & 15;
-  const int ty = threadIdx.x >> 4;
+  __shared__ long long tptr[kUpdMaxFronts + 1];
+  __shared__ long long wsum[kUpdThreads / 32];
+  __shared__ int last;
+  const int tid = threadIdx.x;
+  {
+    // tile counts of the fronts (kUpdMaxFronts / kUpdThreads per thread,
+    // contiguous), then an exclusive scan over the CTA
+    constexpr int per = kUpdMaxFronts / kUpdThreads;
+    long long cnt[per];
+    long long mine = 0;
+#pragma unroll
+    for (int u = 0; u < per; u++) {
+      const int i = tid * per + u;
+      cnt[u] = 0;
+      if (i < nl) {
+        const BigFront& B = s.big[list5[i]];
+        if (B.state != 2 && B.kw > 0) {
+          const long long t = (B.f - B.k + kTile - 1) / kTile;
+          cnt[u] = t * (t + 1) / 2;
+        }
+      }
+      mine += cnt[u];
+    }
+    const int lane = tid & 31;
+    const int w = tid >> 5;
+    long long incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    long long base = 0;
+    for (int q = 0; q < w; q++) base += wsum[q];
+    long long run = base + incl - mine;
+    if (tid == 0) tptr[0] = 0;
+#pragma unroll
+    for (int u = 0; u < per; u++) {
+      run += cnt[u];
+      const int i = tid * per + u;
+      if (i < nl) tptr[i + 1] = run;
+    }
+  }
+  __syncthreads();
+  const long long total = tptr[nl];
+  const int tx = tid & 15;
+  const int ty = tid >> 4;
   for (long long t = blockIdx.x; t < total; t += gridDim.x) {
-    // find the front: last fi with tile_ptr[fi] <= t
-    int lo = 0, hi = nbig;
+    // the front: last fi with tptr[fi] <= t
+    int lo = 0, hi = nl;
     while (hi - lo > 1) {
       const int mid = (lo + hi) >> 1;
-      if (s.tile_ptr[mid] <= t)
+      if (tptr[mid] <= t)
         lo = mid;
       else
         hi = mid;
     }
-    const BigFront& B = s.big[lo];
-    const long long lt = t - s.tile_ptr[lo];
+    const BigFront& B = s.big[list5[lo]];
+    const long long lt = t - tptr[lo];
     int I = (int)((sqrt(8.0 * (double)lt + 1.0) - 1.0) * 0.5);
     while ((long long)(I + 1) * (I + 2) / 2 <= lt) I++;
     while ((long long)I * (I + 1) / 2 > lt) I--;
@@ -608,7 +624,7 @@ __global__ void __launch_bounds__(kUpdThreads) big_update_kernel(DevState s, int
     const int i0 = k + I * kTile;
     const int j0 = k + J * kTile;
     __syncthreads();
-    for (int q = threadIdx.x; q < kw * kTile; q += blockDim.x) {
+    for (int q = tid; q < kw * kTile; q += blockDim.x) {
       const int c = q / kTile;
       const int r = q - c * kTile;
       const int i = i0 + r;
@@ -644,23 +660,28 @@ __global__ void __launch_bounds__(kUpdThreads) big_update_kernel(DevState s, int
       }
     }
   }
-}
-
-__global__ void big_after_update_kernel(DevState s, int nbig) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nbig) return;
-  BigFront& B = s.big[i];
-  if (B.state == 2) return;
-  if (B.kw > 0) {
-    const double r = (double)(B.f - B.k);
-    const double fl = r * (r + 1.0) * B.kw;
-    B.flops += fl;
-    atomicAdd(s.flops + 2, fl);
-    // trailing lower triangle read and written, panel L and W rows read
-    atomicAdd(s.flops + 3, 8.0 * (r * (r + 1.0) + 2.0 * r * B.kw));
+  // close the panel once every CTA is done with the fronts' fields
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = (atomicAdd(reinterpret_cast<unsigned*>(s.err + 2), 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int i = tid; i < nl; i += blockDim.x) {
+    BigFront& B = s.big[list5[i]];
+    if (B.state == 2) continue;
+    if (B.kw > 0) {
+      const double r = (double)(B.f - B.k);
+      const double fl = r * (r + 1.0) * B.kw;
+      B.flops += fl;
+      atomicAdd(s.flops + 2, fl);
+      // trailing lower triangle read and written, panel L and W rows read
+      atomicAdd(s.flops + 3, 8.0 * (r * (r + 1.0) + 2.0 * r * B.kw));
+    }
+    B.kw = 0;
+    if (B.state == 1) B.state = 2;
   }
-  B.kw = 0;
-  if (B.state == 1) B.state = 2;
+  if (tid == 0) s.err[2] = 0;
 }
 
 __global__ void big_finalize_kernel(DevState s, int nbig, int cholesky) {
@@ -787,10 +808,11 @@ cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevel
     if (e != cudaSuccess) return e;
     prof.end(kPhBigPanel, stream, 1);
     prof.begin(stream);
-    big_tiles_kernel<<<1, 1024, 0, stream>>>(s, nb);
-    big_update_kernel<<<upd_grid, kUpdThreads, 0, stream>>>(s, nb);
-    big_after_update_kernel<<<(nb + 255) / 256, 256, 0, stream>>>(s, nb);
-    prof.end(kPhBigUpd, stream, 3);
+    for (int c0 = 0; c0 < info.count_large; c0 += kUpdMaxFronts) {
+      const int nl = std::min(kUpdMaxFronts, info.count_large - c0);
+      big_update_kernel<<<upd_grid, kUpdThreads, 0, stream>>>(s, list5 + c0, nl);
+    }
+    prof.end(kPhBigUpd, stream, (info.count_large + kUpdMaxFronts - 1) / kUpdMaxFronts);
   }
   prof.begin(stream);
   big_finalize_kernel<<<(nb + 255) / 256, 256, 0, stream>>>(s, nb, prm.cholesky);

@@ -134,7 +134,8 @@ struct DevState {
   unsigned long long* used;  // [3]: ints used, doubles used, update rows used
   unsigned long long icap, dcap;
   int64_t* u_off;   // [nn] into the solve's update-vector pool (units of rows)
-  int* err;         // [4]: [0] overflow flag, [1] node of first error
+  int* err;         // [4]: [0] overflow flag, [1] node of first error,
+                    // [2] completion ticket of the trailing-update launch
   int* inertia;     // [2] pos, neg
   double* flops;    // [kWork] executed flops: [0] all fronts, [1] big panels,
                     // [2] big trailing updates, [3] trailing-update bytes
@@ -144,7 +145,6 @@ struct DevState {
                     // class counts [5..9], class max f [10..14]
   int* class_list;  // [6][nn] big-front indices per size class
   int cf_limit[5];  // largest front of each on-chip class
-  long long* tile_ptr;  // [nn+1] update tiles per big front (prefix)
 };
 
 struct FactorParams {
