@@ -113,6 +113,12 @@ struct b200ldl_handle {
   double exec_flops = 0.0;
   int fmax = 0;
   std::vector<int> level_fmax;
+  // solve schedule of the last factorization: per level, the supernodes for
+  // the one-CTA kernels then those for the cluster kernels
+  std::vector<int> solve_ptr;    // [2 * levels + 1]
+  std::vector<int> solve_nodes;  // host copy of d_solve_nodes
+  std::vector<int> solve_fmax;   // [2 * levels]: largest front of each list
+  DevBuf<int> d_solve_nodes;
   Prof prof;
   double flops4[kWork] = {};
   double sum_delayed = 0.0;
@@ -355,6 +361,7 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
   if (!configured) {
     CK(configure_factor_kernels());
     CK(configure_solve_kernels());
+    CK(configure_solve_big_kernels());
     CK(configure_big_kernels());
     configured = true;
   }
@@ -431,13 +438,33 @@ void level_fronts(b200ldl_t h) {
   std::vector<int> f(nn);
   CK(cudaMemcpy(f.data(), h->d_f.ptr, nn * sizeof(int), cudaMemcpyDeviceToHost));
   h->level_fmax.assign(h->num_levels, 1);
+  h->solve_ptr.assign(2 * h->num_levels + 1, 0);
+  h->solve_fmax.assign(2 * h->num_levels, 1);
+  h->solve_nodes.clear();
   int m = 1;
   for (int l = 0; l < h->num_levels; l++) {
+    for (int pass = 0; pass < 2; pass++) {
+      h->solve_ptr[2 * l + pass] = (int)h->solve_nodes.size();
+      for (int q = h->level_ptr[l]; q < h->level_ptr[l + 1]; q++) {
+        const int node = h->hp_level_nodes[q];
+        const int fn = f[node];
+        const bool big = fn >= kSolveBigFront && solve_big_fits(fn);
+        if (big != (pass == 1)) continue;
+        h->solve_nodes.push_back(node);
+        h->solve_fmax[2 * l + pass] = std::max(h->solve_fmax[2 * l + pass], fn);
+        if (!big) m = std::max(m, fn);
+      }
+    }
     for (int q = h->level_ptr[l]; q < h->level_ptr[l + 1]; q++)
       h->level_fmax[l] = std::max(h->level_fmax[l], f[h->hp_level_nodes[q]]);
-    m = std::max(m, h->level_fmax[l]);
   }
-  h->fmax = m;
+  h->solve_ptr[2 * h->num_levels] = (int)h->solve_nodes.size();
+  if (h->d_solve_nodes.count < h->solve_nodes.size())
+    CK(h->d_solve_nodes.alloc(h->solve_nodes.size()));
+  if (!h->solve_nodes.empty())
+    CK(cudaMemcpy(h->d_solve_nodes.ptr, h->solve_nodes.data(),
+                  h->solve_nodes.size() * sizeof(int), cudaMemcpyHostToDevice));
+  h->fmax = m;  // largest front left to the one-CTA kernels
 }
 
 void run_solve(b200ldl_t h, int nrhs, double* x, int ldx) {
@@ -446,20 +473,28 @@ void run_solve(b200ldl_t h, int nrhs, double* x, int ldx) {
     throw std::runtime_error("front too large for the solve kernels");
   const size_t need = (size_t)h->used[2] * nrhs;
   if (h->d_upool.count < need) CK(h->d_upool.alloc(need));
+  const int* nodes = h->d_solve_nodes.ptr;
+  cudaError_t err = cudaSuccess;
   for (int l = 0; l < h->num_levels; l++) {
-    const int b = h->level_ptr[l];
+    const int s0 = h->solve_ptr[2 * l], s1 = h->solve_ptr[2 * l + 1];
+    const int s2 = h->solve_ptr[2 * l + 2];
     h->prof.begin(h->stream);
-    const int nl = launch_forward_level(h->plan, h->st, h->d_level_nodes.ptr + b,
-                                        h->level_ptr[l + 1] - b, x, ldx, nrhs, h->d_upool.ptr,
-                                        h->level_fmax[l], h->stream);
+    int nl = launch_forward_level(h->plan, h->st, nodes + s0, s1 - s0, x, ldx, nrhs,
+                                  h->d_upool.ptr, h->solve_fmax[2 * l], h->stream);
+    nl += launch_forward_big(h->plan, h->st, nodes + s1, s2 - s1, x, ldx, nrhs, h->d_upool.ptr,
+                             h->solve_fmax[2 * l + 1], h->stream, &err);
+    CK(err);
     h->prof.end(kPhFwd, h->stream, nl);
   }
   for (int l = h->num_levels - 1; l >= 0; l--) {
-    const int b = h->level_ptr[l];
+    const int s0 = h->solve_ptr[2 * l], s1 = h->solve_ptr[2 * l + 1];
+    const int s2 = h->solve_ptr[2 * l + 2];
     h->prof.begin(h->stream);
-    const int nl = launch_backward_level(h->plan, h->st, h->d_level_nodes.ptr + b,
-                                         h->level_ptr[l + 1] - b, x, ldx, nrhs,
-                                         h->level_fmax[l], h->stream);
+    int nl = launch_backward_level(h->plan, h->st, nodes + s0, s1 - s0, x, ldx, nrhs,
+                                   h->solve_fmax[2 * l], h->stream);
+    nl += launch_backward_big(h->plan, h->st, nodes + s1, s2 - s1, x, ldx, nrhs,
+                              h->solve_fmax[2 * l + 1], h->stream, &err);
+    CK(err);
     h->prof.end(kPhBwd, h->stream, nl);
   }
   CK(cudaGetLastError());

@@ -209,6 +209,18 @@ int launch_backward_level(const DevPlan& p, const DevState& s,
                           int ldx, int nrhs, int fmax, cudaStream_t stream);
 cudaError_t configure_solve_kernels();
 
+// Supernodes with fronts of at least kSolveBigFront rows are solved by a
+// 16-CTA cluster each (solve_big.cu) when their vectors fit its shared memory.
+constexpr int kSolveBigFront = 1536;
+bool solve_big_fits(int f);
+cudaError_t configure_solve_big_kernels();
+int launch_forward_big(const DevPlan& p, const DevState& s, const int* nodes, int count,
+                       double* x, int ldx, int nrhs, double* upool, int fmax,
+                       cudaStream_t stream, cudaError_t* err);
+int launch_backward_big(const DevPlan& p, const DevState& s, const int* nodes, int count,
+                        double* x, int ldx, int nrhs, int fmax, cudaStream_t stream,
+                        cudaError_t* err);
+
 // residuals and refinement helpers (refine.cu)
 int refine_max_rhs();
 void launch_residual(int n, const int* rowp, const int* cols, const double* vals,

@@ -79,8 +79,10 @@ def test_batched_systems_individually():
         _check_system(s)
 
 
-@pytest.mark.parametrize("nel", [8, 16, 32, 64])
+@pytest.mark.parametrize("nel", [8, 16, 32, 64, 128])
 def test_plane_stress_delayed_pivots(nel):
+    # 128: fronts up to ~3200 rows exercise the chained big-front panels in
+    # HBM, the tiled trailing update and the cluster solves of big supernodes
     g, r = _check_system(plane_stress_kkt(nel))
     npiv_g, ndel_g = g.node_pivots()
     npiv_r, ndel_r = r.node_pivots()
