@@ -546,7 +546,7 @@ __global__ void __launch_bounds__(kPanelThreads)
 // them): lower-triangular 64x64 tiles of each front's trailing matrix in one
 // tile space; every CTA forms the prefix of tile counts itself. The last CTA
 // to finish closes the panel (work counters, kw = 0, finished fronts done).
-__global__ void __launch_bounds__(kUpdThreads)
+__global__ void __launch_bounds__(kUpdThreads, 2)
     big_update_kernel(DevState s, const int* __restrict__ list5, int nl) {
   __shared__ double As[kBigPanelMax][kTile];
   __shared__ double Bs[kBigPanelMax][kTile];
@@ -623,6 +623,18 @@ __global__ void __launch_bounds__(kUpdThreads)
     const double* W = s.dpool + B.woff;
     const int i0 = k + I * kTile;
     const int j0 = k + J * kTile;
+    // this thread's 4x4 entries of the trailing tile, loaded first so that
+    // their latency overlaps the panel loads and the products
+    double cur[4][4];
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      const int j = j0 + ty + 16 * b;
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const int i = i0 + tx + 16 * a;
+        cur[a][b] = (j < f && i < f && i >= j) ? F[i + (size_t)f * j] : 0.0;
+      }
+    }
     __syncthreads();
     for (int q = tid; q < kw * kTile; q += blockDim.x) {
       const int c = q / kTile;
@@ -656,7 +668,7 @@ __global__ void __launch_bounds__(kUpdThreads)
 #pragma unroll
       for (int a = 0; a < 4; a++) {
         const int i = i0 + tx + 16 * a;
-        if (i < f && i >= j) F[i + (size_t)f * j] -= acc[a][b];
+        if (i < f && i >= j) F[i + (size_t)f * j] = cur[a][b] - acc[a][b];
       }
     }
   }
