@@ -44,6 +44,13 @@ SIGNATURES = {
     "b200ldl_work": (ctypes.c_int, [_vp, _f64p, ctypes.c_int]),
     "b200ldl_dense_solve_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int, _vp,
                                                    ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "b200ldl_create_batch": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, _i32p, _i32p,
+                                            _i32p, _i32p, ctypes.c_int, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_double, ctypes.c_int]),
+    "b200ldl_num_systems": (ctypes.c_int, [_vp]),
+    "b200ldl_system_inertia": (ctypes.c_int, [_vp, _i32p, _i32p]),
+    "b200ldl_value_gradient": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, _vp,
+                                              ctypes.c_int, _vp, _vp]),
 }
 
 

@@ -76,6 +76,11 @@ struct b200ldl_handle {
 
   Symbolic sym;
   bool uploaded = false;
+  // independent systems factored as one forest (1 for a single system)
+  int nsys = 1;
+  std::vector<int> node_sys;     // [num_nodes] system of each supernode
+  std::vector<int> sys_inertia;  // [2 nsys] after a factorization
+  DevBuf<int> d_node_sys, d_sys_inertia;
   std::vector<int> h_rowp, h_cols;  // the pattern, for residuals
   DevBuf<int> d_rowp, d_cols;
   DevBuf<double> d_refine, d_norms;
@@ -420,6 +425,18 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
     h->exec_flops = h->flops4[0];
     h->prof.collect();
     if (err[0] == 0) {
+      if (h->nsys > 1 && h->solver_type != B200LDL_CHOLESKY) {
+        if (h->d_node_sys.count < h->node_sys.size()) CK(h->d_node_sys.upload(h->node_sys));
+        if (h->d_sys_inertia.count < (size_t)2 * h->nsys) CK(h->d_sys_inertia.alloc(2 * h->nsys));
+        CK(cudaMemsetAsync(h->d_sys_inertia.ptr, 0, 2 * h->nsys * sizeof(int), h->stream));
+        launch_system_inertia(h->st, h->d_node_sys.ptr, h->sym.num_nodes, h->d_sys_inertia.ptr,
+                              h->stream);
+        CK(cudaGetLastError());
+        h->sys_inertia.assign(2 * h->nsys, 0);
+        CK(cudaMemcpyAsync(h->sys_inertia.data(), h->d_sys_inertia.ptr,
+                           2 * h->nsys * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+      }
       h->factored = true;
       return;
     }
@@ -553,6 +570,107 @@ int b200ldl_create(b200ldl_t* out, int n, int nnz, const int* rowp, const int* c
     return st;
   }
   *out = h.release();
+  return 0;
+}
+
+int b200ldl_create_batch(b200ldl_t* out, int nsys, const int* sys_n, const int* sys_nnz,
+                         const int* rowp_cat, const int* cols_cat, int solver_type,
+                         double ustab, double pivot_tol, double delay_growth, int order) {
+  if (!out) return -1;
+  *out = nullptr;
+  if (nsys < 1 || !sys_n || !sys_nnz || !rowp_cat || !cols_cat) return -1;
+  if (solver_type != B200LDL_LDL && solver_type != B200LDL_CHOLESKY) return -1;
+  if (order < 0 || order > 3 || order == B200LDL_ORDER_MULTI_COLOR) return -1;
+  // validate every system and build the block-diagonal pattern
+  long long ntot = 0, nztot = 0;
+  {
+    long long ro = 0, co = 0;
+    for (int si = 0; si < nsys; si++) {
+      const int n = sys_n[si], nnz = sys_nnz[si];
+      if (n < 0 || nnz < 0) return -1;
+      const int* rowp = rowp_cat + ro;
+      const int* cols = cols_cat + co;
+      if (rowp[0] != 0 || rowp[n] != nnz) return -1;
+      for (int i = 0; i < n; i++)
+        if (rowp[i + 1] < rowp[i]) return -1;
+      for (int e = 0; e < nnz; e++)
+        if (cols[e] < 0 || cols[e] >= n) return -1;
+      ro += n + 1;
+      co += nnz;
+      ntot += n;
+      nztot += nnz;
+    }
+    if (ntot > 2147483647LL || nztot > 2147483647LL) return -1;
+  }
+  auto h = std::make_unique<b200ldl_handle>();
+  h->n = (int)ntot;
+  h->nnz = (int)nztot;
+  h->solver_type = solver_type;
+  h->ustab = ustab;
+  h->pivot_tol = pivot_tol;
+  h->delay_growth = delay_growth;
+  h->order = order;
+  h->nsys = nsys;
+  int st = guarded(h.get(), [&]() {
+    std::vector<Symbolic> parts(nsys);
+    std::vector<int> rowp_all(ntot + 1, 0), cols_all(nztot);
+    long long ro = 0, co = 0, voff = 0;
+    for (int si = 0; si < nsys; si++) {
+      const int n = sys_n[si], nnz = sys_nnz[si];
+      const int* rowp = rowp_cat + ro;
+      const int* cols = cols_cat + co;
+      parts[si] = analyze(static_cast<Ordering>(order), n, rowp, cols);
+      for (int i = 0; i < n; i++) rowp_all[voff + i + 1] = (int)(co + rowp[i + 1]);
+      for (int e = 0; e < nnz; e++) cols_all[co + e] = (int)(voff + cols[e]);
+      ro += n + 1;
+      co += nnz;
+      voff += n;
+    }
+    h->sym = merge_symbolic(parts, h->node_sys);
+    build_plan(h.get(), rowp_all.data(), cols_all.data());
+    h->h_rowp = std::move(rowp_all);
+    h->h_cols = std::move(cols_all);
+    return 0;
+  });
+  if (st != 0) {
+    std::fprintf(stderr, "b200ldl_create_batch: %s\n", h->last_error.c_str());
+    return st;
+  }
+  *out = h.release();
+  return 0;
+}
+
+int b200ldl_num_systems(b200ldl_t h) { return h ? h->nsys : -1; }
+
+int b200ldl_value_gradient(b200ldl_t h, int nrhs, const double* lam, int ldl, const double* x,
+                           int ldx, double* gvals, double* gdiag) {
+  return guarded(h, [&]() {
+    if (nrhs < 0 || nrhs > refine_max_rhs() || ldl < h->n || ldx < h->n ||
+        (nrhs > 0 && (!lam || !x || (h->nnz > 0 && !gvals))))
+      return fail(h, -1, "bad gradient arguments");
+    if (h->n == 0) return 0;
+    upload_plan(h);
+    launch_value_gradient(h->n, h->d_rowp.ptr, h->d_cols.ptr, lam, ldl, x, ldx, nrhs, gvals,
+                          gdiag, h->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    return 0;
+  });
+}
+
+int b200ldl_system_inertia(b200ldl_t h, int* npos, int* nneg) {
+  if (!h || !npos || !nneg) return -1;
+  if (!h->factored) return fail(h, -5, "inertia requested before a successful factor");
+  if (h->nsys == 1) {
+    npos[0] = h->inertia[0];
+    nneg[0] = h->inertia[1];
+    return 0;
+  }
+  for (int si = 0; si < h->nsys; si++) {
+    const bool have = h->sys_inertia.size() == (size_t)2 * h->nsys;
+    npos[si] = have ? h->sys_inertia[2 * si] : 0;
+    nneg[si] = have ? h->sys_inertia[2 * si + 1] : 0;
+  }
   return 0;
 }
 

@@ -221,8 +221,15 @@ int launch_backward_big(const DevPlan& p, const DevState& s, const int* nodes, i
                         double* x, int ldx, int nrhs, int fmax, cudaStream_t stream,
                         cudaError_t* err);
 
+// per-system inertia of a batch of independent systems (batch.cu)
+void launch_system_inertia(const DevState& s, const int* node_sys, int nn, int* sys_inertia,
+                           cudaStream_t st);
+
 // residuals and refinement helpers (refine.cu)
 int refine_max_rhs();
+void launch_value_gradient(int n, const int* rowp, const int* cols, const double* lam, int ldl,
+                           const double* x, int ldx, int nr, double* gvals, double* gdiag,
+                           cudaStream_t st);
 void launch_residual(int n, const int* rowp, const int* cols, const double* vals,
                      const double* diag, const double* x, int ldx, const double* b, int ldb,
                      double* r, int ldr, int nr, cudaStream_t st);

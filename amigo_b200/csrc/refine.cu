@@ -103,7 +103,47 @@ __global__ void copy_cols_kernel(int n, int nr, const double* __restrict__ src, 
   }
 }
 
+// Derivative of a scalar loss with respect to the CSR values and the
+// diagonal, given the solution x of K x = b and the adjoint lam = K^{-1} g
+// (g = dloss/dx): dloss/dK(i,j) = -sum_r lam(i,r) x(j,r), one warp per row.
+__global__ void value_gradient_kernel(int n, const int* __restrict__ rowp,
+                                      const int* __restrict__ cols,
+                                      const double* __restrict__ lam, int ldl,
+                                      const double* __restrict__ x, int ldx, int nr,
+                                      double* __restrict__ gvals, double* __restrict__ gdiag) {
+  const int lane = threadIdx.x & 31;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= n) return;
+  double li[kMaxR];
+#pragma unroll
+  for (int c = 0; c < kMaxR; c++) li[c] = (c < nr) ? lam[(size_t)ldl * c + row] : 0.0;
+  for (int e = rowp[row] + lane; e < rowp[row + 1]; e += 32) {
+    const int j = cols[e];
+    double g = 0.0;
+#pragma unroll
+    for (int c = 0; c < kMaxR; c++)
+      if (c < nr) g = fma(li[c], x[(size_t)ldx * c + j], g);
+    gvals[e] = -g;
+  }
+  if (gdiag && lane == 0) {
+    double g = 0.0;
+#pragma unroll
+    for (int c = 0; c < kMaxR; c++)
+      if (c < nr) g = fma(li[c], x[(size_t)ldx * c + row], g);
+    gdiag[row] = -g;
+  }
+}
+
 }  // namespace
+
+void launch_value_gradient(int n, const int* rowp, const int* cols, const double* lam, int ldl,
+                           const double* x, int ldx, int nr, double* gvals, double* gdiag,
+                           cudaStream_t st) {
+  const int threads = 256;
+  const int blocks = (int)(((long long)n * 32 + threads - 1) / threads);
+  value_gradient_kernel<<<blocks, threads, 0, st>>>(n, rowp, cols, lam, ldl, x, ldx, nr, gvals,
+                                                    gdiag);
+}
 
 int refine_max_rhs() { return kMaxR; }
 

@@ -51,4 +51,9 @@ void etree_postorder_colcount(int n, const int* rowp, const int* cols,
 // Full symbolic phase.
 Symbolic analyze(Ordering order, int n, const int* rowp, const int* cols);
 
+// Independent systems as one forest: variables, supernodes and contribution
+// rows of each part shifted past the parts before it, every part's roots
+// listed at the end; node_sys[k] = the part supernode k belongs to.
+Symbolic merge_symbolic(const std::vector<Symbolic>& parts, std::vector<int>& node_sys);
+
 }  // namespace b200ldl

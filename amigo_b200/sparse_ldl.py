@@ -21,7 +21,7 @@ import numpy as np
 
 from . import _native
 
-__all__ = ["SolverType", "OrderingType", "CSRMat", "Vector", "SparseLDL"]
+__all__ = ["SolverType", "OrderingType", "CSRMat", "Vector", "SparseLDL", "SparseLDLBatch"]
 
 
 class SolverType(enum.IntEnum):
@@ -266,6 +266,28 @@ class SparseLDL:
         out = x if b.dim() == 2 else x[:, 0]
         return out, berr, iters.value
 
+    def value_gradient(self, lam, x):
+        """Derivatives of a scalar loss through x = K^{-1} b, given the
+        solution ``x`` and the adjoint ``lam = K^{-1} dloss/dx`` (torch CUDA
+        float64 tensors, [n] or [n, k] with k <= 8): returns ``(gvals,
+        gdiag)`` with gvals[e] = -sum_r lam[i, r] x[j, r] for each stored
+        entry e = (i, j) and gdiag[i] = -sum_r lam[i, r] x[i, r]."""
+        import torch
+
+        lam2 = lam if lam.dim() == 2 else lam.unsqueeze(1)
+        x2 = x if x.dim() == 2 else x.unsqueeze(1)
+        lcm = lam2.t().contiguous()  # rows of the transposed copy: column-major n x k
+        xcm = x2.t().contiguous()
+        k = lcm.shape[0]
+        gvals = torch.empty(self.nnz, dtype=torch.float64, device=lam.device)
+        gdiag = torch.empty(self.n, dtype=torch.float64, device=lam.device)
+        self._sync_stream(lcm)
+        st = self._lib.b200ldl_value_gradient(
+            self._h, k, ctypes.c_void_p(lcm.data_ptr()), self.n, ctypes.c_void_p(xcm.data_ptr()),
+            self.n, ctypes.c_void_p(gvals.data_ptr()), ctypes.c_void_p(gdiag.data_ptr()))
+        _native.check(self._h, st, "value_gradient")
+        return gvals, gdiag
+
     def get_inertia(self):
         p = ctypes.c_int()
         q = ctypes.c_int()
@@ -341,3 +363,95 @@ class SparseLDL:
         _native.check(self._h, st, "stats")
         return {"flops": v[0], "L_bytes": v[1], "cb_bytes": v[2], "max_front": int(v[3]),
                 "delayed": int(v[4]), "levels": int(v[5])}
+
+
+class SparseLDLBatch(SparseLDL):
+    """Many independent symmetric systems factored and solved together.
+
+    ``SparseLDLBatch(mats, ...)`` takes a list of CSRMat (each with its own
+    pattern, size and values). Every system gets the symbolic phase it would
+    get alone in ``SparseLDL``; the numeric factorization and the solves run
+    all systems' supernodes level by level in the same launches. Vectors
+    (diagonals, right-hand sides, solutions) are the systems' vectors
+    concatenated in order; ``offsets[s]:offsets[s+1]`` is system s.
+    """
+
+    def __init__(self, mats, solver_type=SolverType.LDL, ustab: float = 0.01,
+                 pivot_tol: float = 1e-14, delay_growth: float = 2.0,
+                 order=OrderingType.NATURAL):
+        self._lib = _native.load()
+        self.mats = list(mats)
+        if not self.mats:
+            raise ValueError("no systems")
+        sys_n = np.array([m.nrows for m in self.mats], dtype=np.int32)
+        sys_nnz = np.array([int(m.rowp[-1]) for m in self.mats], dtype=np.int32)
+        rowp_cat = np.ascontiguousarray(np.concatenate([m.rowp for m in self.mats]),
+                                        dtype=np.int32)
+        cols_cat = np.ascontiguousarray(np.concatenate([m.cols for m in self.mats]),
+                                        dtype=np.int32)
+        self.offsets = np.concatenate([[0], np.cumsum(sys_n)]).astype(np.int64)
+        self.val_offsets = np.concatenate([[0], np.cumsum(sys_nnz)]).astype(np.int64)
+        self.n = int(self.offsets[-1])
+        self.nnz = int(self.val_offsets[-1])
+        self.solver_type = SolverType(int(solver_type))
+        self.order = int(order)
+        h = ctypes.c_void_p()
+        st = self._lib.b200ldl_create_batch(
+            ctypes.byref(h), len(self.mats), sys_n.ctypes.data_as(_native._i32p),
+            sys_nnz.ctypes.data_as(_native._i32p), rowp_cat.ctypes.data_as(_native._i32p),
+            cols_cat.ctypes.data_as(_native._i32p), int(self.solver_type), float(ustab),
+            float(pivot_tol), float(delay_growth), self.order)
+        if st != 0:
+            raise _native.NativeError(f"b200ldl_create_batch failed with status {st}", st)
+        self._h = h
+        self._keep = []
+        # the block-diagonal pattern, as one CSRMat for the inherited methods
+        rowp_all = np.zeros(self.n + 1, dtype=np.int32)
+        cols_all = np.empty(self.nnz, dtype=np.int32)
+        for i, m in enumerate(self.mats):
+            o, vo = int(self.offsets[i]), int(self.val_offsets[i])
+            rowp_all[o + 1:o + m.nrows + 1] = vo + m.rowp[1:]
+            cols_all[vo:vo + int(m.rowp[-1])] = o + m.cols
+        self.rowp, self.cols = rowp_all, cols_all
+        self.mat = CSRMat(self.n, self.n, rowp_all, cols_all, self._gather_values())
+
+    @property
+    def num_systems(self) -> int:
+        return len(self.mats)
+
+    def _gather_values(self):
+        vals = [_values_of(m) for m in self.mats]
+        if any(_is_torch(v) and v.is_cuda for v in vals):
+            import torch
+
+            dev = next(v.device for v in vals if _is_torch(v) and v.is_cuda)
+            return torch.cat([torch.as_tensor(v, dtype=torch.float64, device=dev) for v in vals])
+        return np.concatenate([np.asarray(v.cpu().numpy() if _is_torch(v) else v, np.float64)
+                               for v in vals])
+
+    def factor(self, diagonal=None) -> int:
+        """Factor every system with its current values; ``diagonal`` is the
+        concatenated diagonal vector (or a list of per-system vectors)."""
+        self.mat.vals = self._gather_values()
+        if isinstance(diagonal, (list, tuple)):
+            parts = [_values_of(d) for d in diagonal]
+            if any(_is_torch(d) for d in parts):
+                import torch
+
+                diagonal = torch.cat([torch.as_tensor(d, dtype=torch.float64) for d in parts])
+            else:
+                diagonal = np.concatenate([np.asarray(d, np.float64) for d in parts])
+        return super().factor(diagonal)
+
+    def system_inertia(self) -> list:
+        ns = len(self.mats)
+        p = np.zeros(ns, np.int32)
+        q = np.zeros(ns, np.int32)
+        st = self._lib.b200ldl_system_inertia(self._h, p.ctypes.data_as(_native._i32p),
+                                              q.ctypes.data_as(_native._i32p))
+        _native.check(self._h, st, "system_inertia")
+        return [(int(a), int(b)) for a, b in zip(p, q)]
+
+    def split(self, x):
+        """Per-system views of a concatenated vector or [n, k] array."""
+        return [x[int(self.offsets[i]):int(self.offsets[i + 1])] for i in range(len(self.mats))]

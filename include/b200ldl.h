@@ -97,6 +97,38 @@ int b200ldl_solve_refine(b200ldl_t h, const double* vals, const double* diag,
  * SparseLDL::get_inertia (include/sparse_ldl.h:205-213). */
 int b200ldl_get_inertia(b200ldl_t h, int* npos, int* nneg);
 
+/* Many independent systems in one handle, factored and solved together
+ * (one level-scheduled forest). The reference factors them one at a time,
+ * each with its own SparseLDL (include/sparse_ldl.h:65-118); each system
+ * here gets the same symbolic phase as it would alone. sys_n[s], sys_nnz[s]:
+ * size and nonzeros of system s; rowp_cat: the systems' CSR row pointers
+ * one after another (n_s + 1 entries each, local offsets); cols_cat: their
+ * column indices one after another (local indices). b200ldl_factor and
+ * b200ldl_solve then take the systems' values, diagonals and right-hand
+ * sides concatenated in the same order (total size sum n_s). */
+int b200ldl_create_batch(b200ldl_t* out, int nsys, const int* sys_n, const int* sys_nnz,
+                         const int* rowp_cat, const int* cols_cat, int solver_type,
+                         double ustab, double pivot_tol, double delay_growth, int order);
+
+/* Derivatives of a scalar loss through x = K^{-1} b (no counterpart in the
+ * reference, which differentiates post-optimality with extra solves on the
+ * host, amigo/algorithm/ipm_driver.py:297-353): given the solution x and the
+ * adjoint lam = K^{-1} (dloss/dx) from b200ldl_solve on the same factor,
+ * writes gvals[e] = -sum_r lam(i,r) x(j,r) for every stored entry e = (i,j)
+ * of the CSR pattern and, if gdiag is not NULL, gdiag[i] = -sum_r lam(i,r)
+ * x(i,r). dloss/db is lam itself. Device pointers, nrhs <= 8. For values
+ * that are kept symmetric (K(i,j) and K(j,i) from the same parameter) the
+ * entry-wise gradients sum to the exact derivative. */
+int b200ldl_value_gradient(b200ldl_t h, int nrhs, const double* lam, int ldl, const double* x,
+                           int ldx, double* gvals, double* gdiag);
+
+/* Number of systems in the handle (1 for b200ldl_create). */
+int b200ldl_num_systems(b200ldl_t h);
+
+/* Inertia of every system of the last factorization (arrays of
+ * b200ldl_num_systems entries), with get_inertia's counting rule. */
+int b200ldl_system_inertia(b200ldl_t h, int* npos, int* nneg);
+
 /* Message for the last non-zero status on this handle ("" if none). */
 const char* b200ldl_last_error(b200ldl_t h);
 
