@@ -262,7 +262,7 @@ void build_plan(b200ldl_t h, const int* rowp, const int* cols) {
     ints += 2.0 * f;
     dbl += f * h->h_ns[k] + (double)h->h_nc[k] * h->h_nc[k];
     if (f > kSmemFrontMax) dbl += f * f + 2.0 * f;
-    if (f > cluster_front_limit(4)) dbl += f * f;  // permutation scratch of the chained panels
+    if (f > cluster_front_limit(4)) dbl += f * f + 32.0 * f;  // chained panels' scratch
   }
   const double g = std::max(1.0, h->delay_growth);
   h->icap = (unsigned long long)(ints * g * 1.5) + (1u << 16);

@@ -806,13 +806,15 @@ cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevel
     prof.end(kPhBigAsm, stream, 2 + (diag ? 1 : 0) + maxkids);
   }
   const int upd_grid = 148 * 4;
-  const bool chained = big_chain_fits(info.max_f_large);
-  const int nsteps = chained ? (info.max_fs_large + kChainPanel - 2) / (kChainPanel - 1) + 1 : steps;
+  const int cnb = big_chain_panel_width(info.max_f_large);
+  const bool chained = cnb > 0;
+  const int nsteps = chained ? (info.max_fs_large + cnb - 2) / (cnb - 1) + 1 : steps;
   for (int st = 0; st < nsteps; st++) {
     cudaError_t e;
     prof.begin(stream);
     if (chained)
-      e = launch_big_chain_panel(s, prm, info.count_large, info.max_f_large, list5, stream);
+      e = launch_big_chain_panel(s, prm, info.count_large, info.max_f_large, cnb, list5,
+                                 stream);
     else if (CL == 16)
       e = launch_panel<16>(s, prm, info.count_large, NB, smem, list5, stream);
     else

@@ -33,22 +33,24 @@ using namespace chain;
 constexpr int kBcCL = 16;
 constexpr int kBcThreads = 256;
 constexpr int kBcWarps = kBcThreads / 32;
-constexpr int kNB = kChainPanel;  // panel width
-constexpr int kNBP = kNB + 1;     // odd row stride of the panel's L
 static_assert(kChain == kBcWarps, "one chain member per warp");
 
+// panel width NB: 32 where the panel state fits, 16 for the largest fronts
+template <int NB>
 struct BcShared {
   ChainXchg<kBcCL, 2> x;
-  int piv[kNB];  // physical rows of the panel's pivots
+  int piv[NB];  // physical rows of the panel's pivots
   int scan[kBcWarps];
 };
 
-// Shared-memory layout (bytes): the panel's L for own rows [R][kNBP]
-// doubles, the chain's columns over own rows [2][2][kChain][R] doubles,
-// then perm and ipos [f] as 16-bit indices and the moved positions [f].
+// Shared-memory layout (bytes): the panel's L for own rows [R][NB + 1]
+// doubles (odd row stride), the chain's columns over own rows
+// [2][2][kChain][R] doubles, then perm and ipos [f] as 16-bit indices and
+// the moved positions [f].
+template <int NB>
 __host__ __device__ __forceinline__ size_t bc_smem(int f) {
   const size_t R = (size_t)(f + kBcCL - 1) / kBcCL;
-  return R * kNBP * 8 + (size_t)4 * kChain * R * 8 + (size_t)3 * f * 2 + 16;
+  return R * (NB + 1) * 8 + (size_t)4 * kChain * R * 8 + (size_t)3 * f * 2 + 16;
 }
 
 template <typename T>
@@ -66,11 +68,13 @@ __device__ __forceinline__ double fsym(const double* F, int f, int a, int b) {
 // per lane pass so that their HBM loads are in flight together (more rows
 // in flight measured slower: the strided loads of the row part queue up).
 constexpr int kRowsPerLane = 4;
-template <typename Use>
+template <int NB, typename Use>
 __device__ __forceinline__ void big_member_column(const double* F, int f, const double* Lp,
                                                   const unsigned short* ipos, int r0, int Q,
                                                   int pc, int k, int lane, const double* w,
                                                   double* out, Use use) {
+  constexpr int kNB = NB;
+  constexpr int kNBP = NB + 1;
   for (int qb = lane; qb < Q; qb += 32 * kRowsPerLane) {
     double fv4[kRowsPerLane];
     int pos4[kRowsPerLane];
@@ -104,13 +108,16 @@ __device__ __forceinline__ void big_member_column(const double* F, int f, const 
   __syncwarp();
 }
 
+template <int NB>
 __global__ void __launch_bounds__(kBcThreads)
     big_chain_panel_kernel(DevState s, FactorParams prm, const int* __restrict__ list) {
+  constexpr int kNB = NB;
+  constexpr int kNBP = NB + 1;
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
   BigFront* B = s.big + list[blockIdx.x / kBcCL];
   extern __shared__ __align__(16) double sm[];
-  __shared__ BcShared sh;
+  __shared__ BcShared<NB> sh;
   if (B->state != 0) return;  // the same in every CTA of the cluster
 
   const int tid = threadIdx.x;
@@ -131,9 +138,9 @@ __global__ void __launch_bounds__(kBcThreads)
   unsigned short* ipos = perm + f;
   unsigned short* mlist = ipos + f;
   double* F = s.dpool + B->doff;
-  double* Wg = s.dpool + B->woff;        // [kNB][f] logical, for the trailing update
-  double* Wph = Wg + (size_t)kNB * f;    // [kNB][f] by physical row, inside the panel
-  double* T = Wph + (size_t)kNB * f;     // permutation scratch [fs + 1][f]
+  double* Wg = s.dpool + B->woff;                 // [NB][f] logical, for the trailing update
+  double* Wph = Wg + (size_t)kBigPanelMax * f;    // [NB][f] by physical row, inside the panel
+  double* T = Wph + (size_t)kBigPanelMax * f;     // permutation scratch [fs + 1][f]
   int* fv = s.ivars + B->ioff;
   int* orig = fv + f;
 
@@ -182,7 +189,7 @@ __global__ void __launch_bounds__(kBcThreads)
       double bv = 0.0, cm = 0.0;
       int bi = INT_MAX;
       double* out = cb0 + (size_t)t * R;
-      big_member_column(F, f, Lp, ipos, r0, Q, pc, k, lane, w, out,
+      big_member_column<NB>(F, f, Lp, ipos, r0, Q, pc, k, lane, w, out,
                         [&](int q, int r, int pos, double v) {
                           int j = -1;
                           if (pos == k)
@@ -229,7 +236,7 @@ __global__ void __launch_bounds__(kBcThreads)
         double rm = 0.0;
         double* out = cb1 + (size_t)t * R;
         const double* colk = cb0 + (size_t)t * R;
-        big_member_column(F, f, Lp, ipos, r0, Q, pc, k, lane, w, out,
+        big_member_column<NB>(F, f, Lp, ipos, r0, Q, pc, k, lane, w, out,
                           [&](int q, int r, int pos, double v) {
                             if (r == pc) {
                               const double wik = colk[q];
@@ -425,29 +432,28 @@ __global__ void __launch_bounds__(kBcThreads)
   cl.sync();
 }
 
-}  // namespace
-
-size_t big_chain_smem(int f) { return bc_smem(f); }
-
-bool big_chain_fits(int f) {
-  return f <= 65535 && bc_smem(f) + sizeof(BcShared) + 1024 <= 232448;
+template <int NB>
+bool fits(int f) {
+  return f <= 65535 && bc_smem<NB>(f) + sizeof(BcShared<NB>) + 1024 <= 232448;
 }
 
-cudaError_t configure_big_chain_kernel() {
-  cudaError_t e = cudaFuncSetAttribute(big_chain_panel_kernel,
+template <int NB>
+cudaError_t configure_nb() {
+  cudaError_t e = cudaFuncSetAttribute(big_chain_panel_kernel<NB>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(232448 - sizeof(BcShared) - 1024));
+                                       (int)(232448 - sizeof(BcShared<NB>) - 1024));
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(big_chain_panel_kernel,
+  return cudaFuncSetAttribute(big_chain_panel_kernel<NB>,
                               cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
 }
 
-cudaError_t launch_big_chain_panel(const DevState& s, const FactorParams& prm, int count,
-                                   int max_f, const int* list, cudaStream_t stream) {
+template <int NB>
+cudaError_t launch_nb(const DevState& s, const FactorParams& prm, int count, int max_f,
+                      const int* list, cudaStream_t stream) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(count * kBcCL, 1, 1);
   cfg.blockDim = dim3(kBcThreads, 1, 1);
-  cfg.dynamicSmemBytes = bc_smem(max_f);
+  cfg.dynamicSmemBytes = bc_smem<NB>(max_f);
   cfg.stream = stream;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -456,7 +462,27 @@ cudaError_t launch_big_chain_panel(const DevState& s, const FactorParams& prm, i
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, big_chain_panel_kernel, s, prm, list);
+  return cudaLaunchKernelEx(&cfg, big_chain_panel_kernel<NB>, s, prm, list);
+}
+
+}  // namespace
+
+int big_chain_panel_width(int f) {
+  if (fits<32>(f)) return 32;
+  if (fits<16>(f)) return 16;
+  return 0;
+}
+
+cudaError_t configure_big_chain_kernel() {
+  cudaError_t e = configure_nb<16>();
+  if (e != cudaSuccess) return e;
+  return configure_nb<32>();
+}
+
+cudaError_t launch_big_chain_panel(const DevState& s, const FactorParams& prm, int count,
+                                   int max_f, int nb, const int* list, cudaStream_t stream) {
+  return nb == 32 ? launch_nb<32>(s, prm, count, max_f, list, stream)
+                  : launch_nb<16>(s, prm, count, max_f, list, stream);
 }
 
 }  // namespace b200ldl

@@ -153,9 +153,11 @@ __global__ void __launch_bounds__(kFactorThreads)
     sh_ioff = (long long)io;
     if (big) {
       // the front itself plus the panel's W columns; fronts above the
-      // on-chip limit also get the chained panel's permutation scratch
+      // on-chip limit also get the chained panel's W by physical row and its
+      // permutation scratch
       unsigned long long need = (unsigned long long)f * f + (unsigned long long)kBigPanelMax * f;
-      if (f > s.cf_limit[4]) need += (unsigned long long)(fs + 1) * f;
+      if (f > s.cf_limit[4])
+        need += (unsigned long long)kBigPanelMax * f + (unsigned long long)(fs + 1) * f;
       const unsigned long long dofs = atomicAdd(s.used + 1, need);
       if (dofs + need > s.dcap) fail = 1;
       sh_doff = (long long)dofs;

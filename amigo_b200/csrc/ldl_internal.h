@@ -116,7 +116,6 @@ struct BigFront {
 };
 
 constexpr int kBigPanelMax = 32;
-constexpr int kChainPanel = 16;  // panel width of the chained big-front kernel
 
 // Mutable state of one factorization (device memory).
 struct DevState {
@@ -185,10 +184,12 @@ cudaError_t launch_cluster_fronts(const DevPlan& p, const DevState& s, const int
                                   const FactorParams& prm, cudaStream_t stream, int nn);
 // Class-5 fronts whose panel state fits one cluster's shared memory use the
 // chained panel kernel (big_chain.cu); larger ones the single-candidate one.
-bool big_chain_fits(int f);
+// Panel width (32 or 16) the chained kernel uses for fronts up to f, 0 if
+// its panel state does not fit.
+int big_chain_panel_width(int f);
 cudaError_t configure_big_chain_kernel();
 cudaError_t launch_big_chain_panel(const DevState& s, const FactorParams& prm, int count,
-                                   int max_f, const int* list, cudaStream_t stream);
+                                   int max_f, int nb, const int* list, cudaStream_t stream);
 
 cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
                              int maxkids, const FactorParams& prm, const double* vals,

@@ -402,6 +402,87 @@ def run_ours(args, world, rank, local):
     return 0
 
 
+def run_batched(args, world, rank, local):
+    """Secondary workload: many independent optimal-control KKT systems of
+    uneven size (N ~ U{50..400}, nx = 6, nu = 3, one RHS each), factored and
+    solved together in one handle. One step = factor + solve of all systems.
+    Not the headline metric; printed in the same JSON shape."""
+    import torch
+
+    from amigo_b200.sparse_ldl import CSRMat, OrderingType, SparseLDLBatch, Vector
+    from amigo_b200.workloads import batched_optimal_control
+
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    systems = batched_optimal_control(num_systems=args.systems, seed=0)
+    mats = [CSRMat(q.n, q.n, q.rowp, q.cols, torch.as_tensor(q.vals, device=dev))
+            for q in systems]
+    batch = SparseLDLBatch(mats, order=OrderingType.AMD)
+    diag = Vector(torch.as_tensor(np.concatenate([q.diag for q in systems]), device=dev))
+    bh = np.concatenate([q.rhs[:, 0] for q in systems])
+    b = torch.as_tensor(bh, device=dev)
+    x = torch.empty_like(b)
+
+    def step():
+        batch.factor(diag)
+        x.copy_(b)
+        batch.solve(x)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    launches0 = batch.launch_count()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = batch.launch_count() - launches0
+    xh = x.cpu().numpy()
+    berr = max(backward_error(q, xs.reshape(-1, 1), q.rhs[:, :1])
+               for q, xs in zip(systems, batch.split(xh)))
+    inertia = batch.system_inertia()
+    ok = all(tuple(i) == q.expected_inertia for i, q in zip(inertia, systems))
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import ref
+
+        if ref.available():
+            # serial reference, one system after another, on a bounded sample
+            t_all, done, n_done = time.perf_counter(), 0.0, 0
+            for q in systems:
+                r = ref.RefLDL(q.rowp, q.cols, order=ref.ORDER_AMD)
+                t0 = time.perf_counter()
+                r.factor(q.vals, q.diag)
+                r.solve(q.rhs[:, :1])
+                done += time.perf_counter() - t0
+                r.close()
+                n_done += 1
+                if time.perf_counter() - t_all > 20.0:
+                    break
+            per_batch = done / n_done * len(systems)
+            cpu = {"value": 1.0 / per_batch, "unit": "batch factor+solve/s", "cores": 1,
+                   "kind": "reference",
+                   "sample": f"{n_done} of {len(systems)} systems, serial, scaled to the batch"}
+    line = {
+        "metric": METRIC, "value": 1e3 / ms, "unit": "batch factor+solve/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"{len(systems)} independent optimal-control KKT systems "
+                               f"(n total {batch.n}), one RHS each, AMD, FP64, one handle",
+                   "systems_per_s": len(systems) * 1e3 / ms},
+        "cpu_baseline": cpu, "gpu_launches": launches, "backward_error": berr,
+        "berr_target_met": bool(berr <= BERR_TARGET), "inertia_all_expected": ok,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -414,8 +495,13 @@ def main(argv=None) -> int:
     ap.add_argument("--no-e2e", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-profile-pass", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-clocks", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--workload", choices=["plane_stress", "batched"], default="plane_stress",
+                    help=argparse.SUPPRESS)
+    ap.add_argument("--systems", type=int, default=512, help=argparse.SUPPRESS)
     args = ap.parse_args(argv)
     world, rank, local = dist_setup()
+    if args.workload == "batched":
+        return run_batched(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, world, rank)
     return run_ours(args, world, rank, local)
