@@ -71,8 +71,8 @@ constexpr int kRowsPerLane = 4;
 template <int NB, typename Use>
 __device__ __forceinline__ void big_member_column(const double* F, int f, const double* Lp,
                                                   const unsigned short* ipos, int r0, int Q,
-                                                  int pc, int k, int lane, const double* w,
-                                                  double* out, Use use) {
+                                                  int pc, int k, int kwn, int lane,
+                                                  const double* w, double* out, Use use) {
   constexpr int kNB = NB;
   constexpr int kNBP = NB + 1;
   for (int qb = lane; qb < Q; qb += 32 * kRowsPerLane) {
@@ -95,10 +95,16 @@ __device__ __forceinline__ void big_member_column(const double* F, int f, const 
       const int q = qb + 32 * u;
       const double* lr = Lp + (size_t)q * kNBP;
       double a0 = 0.0, a1 = 0.0;
+      // columns at and beyond the panel's width are zero: skip them in
+      // groups of 8 (exact, the skipped products are zeros)
 #pragma unroll
-      for (int c = 0; c < kNB; c += 2) {
-        a0 = fma(lr[c], w[c], a0);
-        a1 = fma(lr[c + 1], w[c + 1], a1);
+      for (int c8 = 0; c8 < kNB; c8 += 8) {
+        if (c8 >= kwn) break;
+#pragma unroll
+        for (int c = c8; c < c8 + 8; c += 2) {
+          a0 = fma(lr[c], w[c], a0);
+          a1 = fma(lr[c + 1], w[c + 1], a1);
+        }
       }
       const double v = fv4[u] - (a0 + a1);
       out[q] = v;
@@ -189,7 +195,7 @@ __global__ void __launch_bounds__(kBcThreads)
       double bv = 0.0, cm = 0.0;
       int bi = INT_MAX;
       double* out = cb0 + (size_t)t * R;
-      big_member_column<NB>(F, f, Lp, ipos, r0, Q, pc, k, lane, w, out,
+      big_member_column<NB>(F, f, Lp, ipos, r0, Q, pc, k, kw, lane, w, out,
                         [&](int q, int r, int pos, double v) {
                           int j = -1;
                           if (pos == k)
@@ -236,7 +242,7 @@ __global__ void __launch_bounds__(kBcThreads)
         double rm = 0.0;
         double* out = cb1 + (size_t)t * R;
         const double* colk = cb0 + (size_t)t * R;
-        big_member_column<NB>(F, f, Lp, ipos, r0, Q, pc, k, lane, w, out,
+        big_member_column<NB>(F, f, Lp, ipos, r0, Q, pc, k, kw, lane, w, out,
                           [&](int q, int r, int pos, double v) {
                             if (r == pc) {
                               const double wik = colk[q];

@@ -134,7 +134,7 @@ template <int CL, typename Use>
 __device__ __forceinline__ void member_column(cg::cluster_group& cl, double* tri,
                                               const double* Lp, const double* Wall,
                                               const int* ipos, int rank, int Q, int pc, int k,
-                                              int lane, double* out, Use use) {
+                                              int kwn, int lane, double* out, Use use) {
   double w[kNB];
   const double* wr = Wall + (size_t)pc * kNBP;
 #pragma unroll
@@ -152,12 +152,18 @@ __device__ __forceinline__ void member_column(cg::cluster_group& cl, double* tri
     const double* l0 = Lp + (size_t)q0 * kNBP;
     const double* l1 = Lp + (size_t)(h1 ? q1 : q0) * kNBP;
     double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+    // columns at and beyond the panel's width are zero: skip them in
+    // groups of 8 (exact, the skipped products are zeros)
 #pragma unroll
-    for (int c = 0; c < kNB; c += 2) {
-      a0 = fma(l0[c], w[c], a0);
-      a1 = fma(l0[c + 1], w[c + 1], a1);
-      b0 = fma(l1[c], w[c], b0);
-      b1 = fma(l1[c + 1], w[c + 1], b1);
+    for (int c8 = 0; c8 < kNB; c8 += 8) {
+      if (c8 >= kwn) break;
+#pragma unroll
+      for (int c = c8; c < c8 + 8; c += 2) {
+        a0 = fma(l0[c], w[c], a0);
+        a1 = fma(l0[c + 1], w[c + 1], a1);
+        b0 = fma(l1[c], w[c], b0);
+        b1 = fma(l1[c + 1], w[c + 1], b1);
+      }
     }
     const double v0 = f0 - (a0 + a1);
     const double v1 = f1 - (b0 + b1);
@@ -322,7 +328,7 @@ __global__ void __launch_bounds__(kCfThreads)
         double bv = 0.0, cm = 0.0;
         int bi = INT_MAX;
         double* out = cb0 + (size_t)t * Qmax;
-        member_column<CL>(cl, tri, Lp, Wall, ipos, rank, Q, pc, k, lane, out,
+        member_column<CL>(cl, tri, Lp, Wall, ipos, rank, Q, pc, k, kw, lane, out,
                           [&](int q, int r, int pos, double v) {
                             int j = -1;
                             if (pos == k)
@@ -366,7 +372,7 @@ __global__ void __launch_bounds__(kCfThreads)
           double rm = 0.0;
           double* out = cb1 + (size_t)t * Qmax;
           const double* colk = cb0 + (size_t)t * Qmax;
-          member_column<CL>(cl, tri, Lp, Wall, ipos, rank, Q, pc, k, lane, out,
+          member_column<CL>(cl, tri, Lp, Wall, ipos, rank, Q, pc, k, kw, lane, out,
                             [&](int q, int r, int pos, double v) {
                               if (r == pc) {
                                 const double wik = colk[q];
