@@ -212,7 +212,7 @@ cudaError_t configure_solve_kernels();
 
 // Supernodes with fronts of at least kSolveBigFront rows are solved by a
 // 16-CTA cluster each (solve_big.cu) when their vectors fit its shared memory.
-constexpr int kSolveBigFront = 1536;
+constexpr int kSolveBigFront = 1024;
 bool solve_big_fits(int f);
 cudaError_t configure_solve_big_kernels();
 int launch_forward_big(const DevPlan& p, const DevState& s, const int* nodes, int count,
