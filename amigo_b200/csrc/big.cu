@@ -156,19 +156,33 @@ __global__ void big_extend_kernel(DevPlan p, DevState s, int c, const int* __res
       if (p2 >= ns) p2 += nd_in;
     }
     const double* col = cb + (size_t)cld * r2;
-    for (int r1 = r2 + lane; r1 < m; r1 += 32) {
-      int p1;
-      if (r1 < nd) {
-        p1 = off + r1;
-      } else {
-        p1 = cm[r1 - nd];
-        if (p1 >= ns) p1 += nd_in;
+    // four entries per lane pass: their loads (map, value, front) are in
+    // flight together before the read-modify-writes
+    for (int rb = r2 + lane; rb < m; rb += 128) {
+      double* dst[4];
+      double val[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const int r1 = rb + 32 * u;
+        dst[u] = nullptr;
+        if (r1 < m) {
+          int p1;
+          if (r1 < nd) {
+            p1 = off + r1;
+          } else {
+            p1 = cm[r1 - nd];
+            if (p1 >= ns) p1 += nd_in;
+          }
+          dst[u] = (p1 >= p2) ? F + (p1 + (size_t)f * p2) : F + (p2 + (size_t)f * p1);
+          val[u] = col[r1];
+        }
       }
-      const double v = col[r1];
-      if (p1 >= p2)
-        F[p1 + (size_t)f * p2] += v;
-      else
-        F[p2 + (size_t)f * p1] += v;
+      double old[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) old[u] = dst[u] ? *dst[u] : 0.0;
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        if (dst[u]) *dst[u] = old[u] + val[u];
     }
   }
 }

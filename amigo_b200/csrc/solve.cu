@@ -37,11 +37,19 @@ __device__ __forceinline__ void gemv_t_col(const double* L, int ldl, int j, int 
   double acc[kMaxRhs];
 #pragma unroll
   for (int r = 0; r < kMaxRhs; r++) acc[r] = 0.0;
-  for (int i = i0 + lane; i < i1; i += 32) {
-    const double l = lj[i];
+  // four rows per lane pass: their loads are in flight together
+  for (int ib = i0 + lane; ib < i1; ib += 128) {
+    double l4[4];
 #pragma unroll
-    for (int r = 0; r < kMaxRhs; r++)
-      if (r < nr) acc[r] += l * v[(size_t)r * f + i];
+    for (int u = 0; u < 4; u++) l4[u] = (ib + 32 * u < i1) ? lj[ib + 32 * u] : 0.0;
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const int i = ib + 32 * u;
+      if (i >= i1) break;
+#pragma unroll
+      for (int r = 0; r < kMaxRhs; r++)
+        if (r < nr) acc[r] += l4[u] * v[(size_t)r * f + i];
+    }
   }
 #pragma unroll
   for (int r = 0; r < kMaxRhs; r++) {
@@ -166,7 +174,7 @@ __device__ __forceinline__ void bwd_block(const double* L, int ldl, const int* f
     if (mine && r < nr) v[(size_t)r * f + jb + lane] = vr[r];
 }
 
-__global__ void __launch_bounds__(kSolveThreads)
+__global__ void __launch_bounds__(kSolveThreads, 2)
     forward_level_kernel(DevPlan p, DevState s, const int* __restrict__ nodes,
                          double* __restrict__ x, int ldx, int nrhs, int r0, int nr,
                          double* __restrict__ upool) {
@@ -232,11 +240,23 @@ __global__ void __launch_bounds__(kSolveThreads)
       double acc[kMaxRhs];
 #pragma unroll
       for (int r = 0; r < kMaxRhs; r++) acc[r] = 0.0;
-      for (int j = jb; j < je; j++) {
-        const double l = L[i + (size_t)ldl * j];
+      // the row's block entries are all loaded before the products, so that
+      // their HBM latency is paid once per row, not once per column
+      // (two halves of 16 columns keep the registers for two CTAs per SM)
 #pragma unroll
-        for (int r = 0; r < kMaxRhs; r++)
-          if (r < nr) acc[r] = fma(l, v[(size_t)r * f + j], acc[r]);
+      for (int h = 0; h < kBlk; h += 16) {
+        if (jb + h >= je) break;
+        double lv[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++)
+          lv[j] = (jb + h + j < je) ? L[i + (size_t)ldl * (jb + h + j)] : 0.0;
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          if (jb + h + j >= je) break;
+#pragma unroll
+          for (int r = 0; r < kMaxRhs; r++)
+            if (r < nr) acc[r] = fma(lv[j], v[(size_t)r * f + jb + h + j], acc[r]);
+        }
       }
 #pragma unroll
       for (int r = 0; r < kMaxRhs; r++)

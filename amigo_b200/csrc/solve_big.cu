@@ -194,9 +194,14 @@ __global__ void __launch_bounds__(kSbThreads)
 #pragma unroll
       for (int r = 0; r < kSbRhs; r++) acc[r] = 0.0;
       const double* li = L + i + (size_t)ldl * jb;
-      for (int j = 0; j < nb; j++) {
-        double l = li[(size_t)ldl * j];
-        if (i == skip_i && j == nb - 1) l = 0.0;
+      // the row's tile entries are all loaded before the products, so that
+      // their HBM latency is paid once per row, not once per column
+      double lv[kTileR];
+#pragma unroll
+      for (int j = 0; j < kTileR; j++) lv[j] = (j < nb) ? li[(size_t)ldl * j] : 0.0;
+#pragma unroll
+      for (int j = 0; j < kTileR; j++) {
+        const double l = (i == skip_i && j == nb - 1) ? 0.0 : lv[j];
 #pragma unroll
         for (int r = 0; r < kSbRhs; r++)
           if (r < nr) acc[r] = fma(l, tb[j * kSbRhs + r], acc[r]);
@@ -308,18 +313,29 @@ __global__ void __launch_bounds__(kSbThreads)
       for (int c = 0; c < 4; c++)
 #pragma unroll
         for (int r = 0; r < kSbRhs; r++) acc[c][r] = 0.0;
-      for (int i = max(je, rb) + lane; i < re; i += 32) {
-        double xv[kSbRhs];
+      // four rows per lane pass: their 16 HBM loads are in flight together
+      for (int ib = max(je, rb) + lane; ib < re; ib += 128) {
+        double lv[4][4];
 #pragma unroll
-        for (int r = 0; r < kSbRhs; r++) xv[r] = (r < nr) ? v[(size_t)r * R + (i - rb)] : 0.0;
+        for (int u = 0; u < 4; u++) {
+          const int i = ib + 32 * u;
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-          const int j = j0 + c;
-          if (j < nb) {
-            double l = L[i + (size_t)ldl * (jb + j)];
-            if (i == skip_i && j == nb - 1) l = 0.0;
+          for (int c = 0; c < 4; c++) {
+            const int j = j0 + c;
+            lv[u][c] = (i < re && j < nb && !(i == skip_i && j == nb - 1))
+                           ? L[i + (size_t)ldl * (jb + j)]
+                           : 0.0;
+          }
+        }
 #pragma unroll
-            for (int r = 0; r < kSbRhs; r++) acc[c][r] = fma(l, xv[r], acc[c][r]);
+        for (int u = 0; u < 4; u++) {
+          const int i = ib + 32 * u;
+          if (i >= re) continue;
+#pragma unroll
+          for (int r = 0; r < kSbRhs; r++) {
+            const double xr = (r < nr) ? v[(size_t)r * R + (i - rb)] : 0.0;
+#pragma unroll
+            for (int c = 0; c < 4; c++) acc[c][r] = fma(lv[u][c], xr, acc[c][r]);
           }
         }
       }
