@@ -3,7 +3,8 @@
 //
 // The front F (f x f, column-major, lower triangle) stays in HBM in logical
 // order at panel boundaries. A cluster of 16 CTAs owns one front: CTA r
-// holds the rows [r R, r R + R) of the panel's L in shared memory, and the
+// holds the rows [k0 + r R, k0 + r R + R) of the panel's L in shared memory
+// (k0 the panel's first pivot, R = (f - k0) / 16 rounded up), and the
 // panel's W columns go to HBM by physical row. Inside the panel the logical
 // order (the reference's symm_swap, SparseLDL::factor_front_matrix_block,
 // include/sparse_ldl.h:1316-1553) is a permutation in shared memory, so a
@@ -135,8 +136,12 @@ __global__ void __launch_bounds__(kBcThreads)
   int k = B->k;
   int ncand = B->ncand;
   const int kstart = k;
-  const int R = (f + kBcCL - 1) / kBcCL;
-  const int r0 = rank * R;
+  // rows before kstart are eliminated, and after the previous panel's
+  // permutation pass the remaining ones are exactly [kstart, f): only those
+  // are split over the CTAs, so the per-step work shrinks as the front
+  // progresses
+  const int R = (f - kstart + kBcCL - 1) / kBcCL;
+  const int r0 = kstart + rank * R;
   const int Q = max(0, min(f, r0 + R) - r0);
   double* Lp = sm;                               // [R][kNBP]
   double* colbuf = Lp + (size_t)R * kNBP;        // [2][2][kChain][R]
@@ -185,9 +190,9 @@ __global__ void __launch_bounds__(kBcThreads)
       if (lane < kw_safe) {
         wl = __ldcg(Wph + (size_t)lane * f + pc);
       } else if (lane < kw) {
-        const int o = pc / R;
+        const int o = (pc - kstart) / R;
         const double* src = (lane == kw_safe) ? prevA : prevB;
-        wl = at_rank(cl, src, o, rank)[pc - o * R];
+        wl = at_rank(cl, src, o, rank)[pc - kstart - o * R];
       }
       double w[kNB];
 #pragma unroll
