@@ -92,6 +92,9 @@ struct b200ldl_handle {
   int num_levels = 0;
   std::vector<int> level_ptr;  // host copy
   std::vector<int> level_maxkids;
+  // a level whose fronts cannot exceed the shared-memory limit, whatever the
+  // delays, needs no big-front launch (and no host read-back)
+  std::vector<char> level_may_big;
   std::vector<int> h_ns, h_nc;
 
   // device plan
@@ -236,6 +239,23 @@ void build_plan(b200ldl_t h, const int* rowp, const int* cols) {
   }
   h->num_levels = nl;
   h->level_ptr = lptr;
+  // an upper bound on every front's run-time size: a child delays at most
+  // all of its candidates, so fs <= ns + sum of the children's bounds
+  {
+    std::vector<long long> fsb(nn, 0);
+    std::vector<int> order(nn);
+    for (int k = 0; k < nn; k++) order[k] = k;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return level[a] < level[b]; });
+    for (int k : order) {
+      long long b = ns[k];
+      for (int c = kid_ptr[k]; c < kid_ptr[k + 1]; c++) b += fsb[kids[c]];
+      fsb[k] = b;
+    }
+    h->level_may_big.assign(nl, 0);
+    for (int k = 0; k < nn; k++)
+      if (fsb[k] + nc[k] > kSmemFrontMax) h->level_may_big[level[k]] = 1;
+  }
   h->level_maxkids.assign(nl, 0);
   for (int l = 0; l < nl; l++)
     for (int q = lptr[l]; q < lptr[l + 1]; q++) {
@@ -383,12 +403,14 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
     for (int l = 0; l < h->num_levels; l++) {
       const int b = h->level_ptr[l];
       const int cnt = h->level_ptr[l + 1] - b;
-      CK(cudaMemsetAsync(h->d_big_meta.ptr, 0, 16 * sizeof(int), h->stream));
+      if (h->level_may_big[l])
+        CK(cudaMemsetAsync(h->d_big_meta.ptr, 0, 16 * sizeof(int), h->stream));
       h->prof.begin(h->stream);
       launch_factor_level(h->plan, h->st, h->d_level_nodes.ptr + b, cnt, prm, h->stream,
                           vals, diag);
       h->prof.end(kPhFront, h->stream, 1);
       CK(cudaGetLastError());
+      if (!h->level_may_big[l]) continue;
       int meta[16];
       CK(cudaMemcpyAsync(meta, h->d_big_meta.ptr, 16 * sizeof(int), cudaMemcpyDeviceToHost,
                          h->stream));
