@@ -51,6 +51,11 @@ SIGNATURES = {
     "b200ldl_system_inertia": (ctypes.c_int, [_vp, _i32p, _i32p]),
     "b200ldl_value_gradient": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int, _vp,
                                               ctypes.c_int, _vp, _vp]),
+    "b200ldl_set_perturbation_rows": (ctypes.c_int, [_vp, ctypes.c_int, _i32p, ctypes.c_int,
+                                                     _i32p]),
+    "b200ldl_factor_perturbed": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double,
+                                                ctypes.c_double, _i32p, _i32p]),
+    "b200ldl_copy_perturbed_diagonal": (ctypes.c_int, [_vp, _vp]),
 }
 
 

@@ -4,6 +4,7 @@
 // extend-add maps, level lists), and the device pools of the last
 // factorization. Errors are returned as status codes with a message kept on
 // the handle; nothing aborts.
+#include <cmath>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -111,6 +112,11 @@ struct b200ldl_handle {
   DevBuf<BigFront> d_big;
   DevBuf<int> d_big_meta;
   DevBuf<int> d_class_list;
+  // inertia correction: per row, bit 0 = primal (+delta_x), bit 1 =
+  // constraint (-delta_c); the perturbed diagonal of the last attempt
+  DevBuf<unsigned char> d_pclass;
+  DevBuf<double> d_pdiag;
+  bool have_pclass = false;
   unsigned long long icap = 0, dcap = 0;
   DevState st{};
 
@@ -730,6 +736,65 @@ int b200ldl_factor_host(b200ldl_t h, const double* vals, const double* diag) {
     h->factored = false;
     h->fmax = 0;
     run_factor(h, h->d_vals.ptr, dd);
+    return 0;
+  });
+}
+
+int b200ldl_set_perturbation_rows(b200ldl_t h, int nprimal, const int* primal, int ndual,
+                                  const int* dual) {
+  return guarded(h, [&]() {
+    if (nprimal < 0 || ndual < 0 || (nprimal > 0 && !primal) || (ndual > 0 && !dual))
+      return fail(h, -1, "bad perturbation row lists");
+    std::vector<unsigned char> cls(std::max(1, h->n), 0);
+    for (int t = 0; t < nprimal; t++) {
+      const int i = primal[t];
+      if (i < 0 || i >= h->n) return fail(h, -1, "primal row index out of range");
+      if (cls[i] & 1) return fail(h, -1, "primal row listed twice");
+      cls[i] |= 1;
+    }
+    for (int t = 0; t < ndual; t++) {
+      const int i = dual[t];
+      if (i < 0 || i >= h->n) return fail(h, -1, "constraint row index out of range");
+      if (cls[i] & 2) return fail(h, -1, "constraint row listed twice");
+      cls[i] |= 2;
+    }
+    if (h->d_pclass.count < cls.size()) CK(h->d_pclass.alloc(cls.size()));
+    if (h->d_pdiag.count < cls.size()) CK(h->d_pdiag.alloc(cls.size()));
+    CK(cudaMemcpyAsync(h->d_pclass.ptr, cls.data(), cls.size(), cudaMemcpyHostToDevice,
+                       h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->have_pclass = true;
+    return 0;
+  });
+}
+
+int b200ldl_factor_perturbed(b200ldl_t h, const double* vals, const double* diag,
+                             double delta_x, double delta_c, int* npos, int* nneg) {
+  return guarded(h, [&]() {
+    if (h->nnz > 0 && !vals) return fail(h, -1, "vals is null");
+    if (!h->have_pclass) return fail(h, -1, "perturbation rows not set");
+    if (!(delta_x >= 0.0) || !(delta_c >= 0.0) || std::isinf(delta_x) || std::isinf(delta_c))
+      return fail(h, -1, "perturbations must be finite and non-negative");
+    h->factored = false;
+    h->fmax = 0;
+    if (h->n > 0)
+      launch_perturb_diag(h->n, diag, h->d_pclass.ptr, delta_x, delta_c, h->d_pdiag.ptr,
+                          h->stream);
+    run_factor(h, vals, h->d_pdiag.ptr);
+    if (npos) *npos = h->inertia[0];
+    if (nneg) *nneg = h->inertia[1];
+    return 0;
+  });
+}
+
+int b200ldl_copy_perturbed_diagonal(b200ldl_t h, double* out) {
+  return guarded(h, [&]() {
+    if (!out) return fail(h, -1, "out is null");
+    if (!h->have_pclass) return fail(h, -1, "perturbation rows not set");
+    if (h->n > 0)
+      CK(cudaMemcpyAsync(out, h->d_pdiag.ptr, sizeof(double) * h->n, cudaMemcpyDeviceToDevice,
+                         h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     return 0;
   });
 }

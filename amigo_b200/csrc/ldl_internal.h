@@ -240,5 +240,9 @@ void launch_infnorm(int n, const int* rowp, const int* cols, const double* vals,
 void launch_axpy(int n, int nr, const double* d, int ldd, double* x, int ldx, cudaStream_t st);
 void launch_copy_cols(int n, int nr, const double* src, int lds, double* dst, int ldd,
                       cudaStream_t st);
+// the diagonal of one inertia-correction attempt; cls bit 0 = primal row
+// (+dx), bit 1 = constraint row (-dc)
+void launch_perturb_diag(int n, const double* diag, const unsigned char* cls, double dx,
+                         double dc, double* out, cudaStream_t st);
 
 }  // namespace b200ldl

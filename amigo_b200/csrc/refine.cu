@@ -4,6 +4,7 @@
 // side, with K the full symmetric CSR plus the diagonal vector (what the
 // factorization assembles, sparse_ldl.h:1099-1104). The reference has no
 // refinement; its plugin's comment asks for one (newton_direction.py:6-8).
+#include <algorithm>
 #include <cuda_runtime.h>
 
 #include "ldl_internal.h"
@@ -134,7 +135,31 @@ __global__ void value_gradient_kernel(int n, const int* __restrict__ rowp,
   }
 }
 
+// The regularized diagonal of one inertia-correction attempt:
+// out[i] = diag[i] (+ dx on primal rows when dx > 0) (- dc on constraint
+// rows when dc > 0), the additions in that order, as
+// InertiaCorrector._compute_perturbation makes them
+// (amigo/algorithm/solvers/inertia_correction.py:293-306).
+__global__ void perturb_diag_kernel(int n, const double* __restrict__ diag,
+                                    const unsigned char* __restrict__ cls, double dx, double dc,
+                                    double* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double v = diag ? diag[i] : 0.0;
+    const unsigned char c = cls[i];
+    if (dx > 0.0 && (c & 1)) v += dx;
+    if (dc > 0.0 && (c & 2)) v += -dc;
+    out[i] = v;
+  }
+}
+
 }  // namespace
+
+void launch_perturb_diag(int n, const double* diag, const unsigned char* cls, double dx,
+                         double dc, double* out, cudaStream_t st) {
+  const int threads = 256;
+  const int blocks = std::max(1, std::min((n + threads - 1) / threads, 148 * 8));
+  perturb_diag_kernel<<<blocks, threads, 0, st>>>(n, diag, cls, dx, dc, out);
+}
 
 void launch_value_gradient(int n, const int* rowp, const int* cols, const double* lam, int ldl,
                            const double* x, int ldx, int nr, double* gvals, double* gdiag,

@@ -106,3 +106,27 @@ class B200LdlSolver(LinearSolver):
 
     def set_pivot_tolerance(self, pivtol):
         pass
+
+    # the pivot tolerance of the threshold test is fixed at construction, as
+    # in AmigoSolver (amigo_solver.py:63-64)
+    uses_pivot_tolerance = False
+
+    # -- inertia correction on the device (amigo_b200.inertia_correction) -------
+    def set_perturbation_rows(self, primal, dual):
+        self.ldl.set_perturbation_rows(primal, dual)
+
+    def load_system(self, hessian, diagonal):
+        """Bring the Hessian values and the diagonal to the device once for
+        the attempts that follow."""
+        if hessian is not self.hessian and hessian != self.hessian:
+            raise ValueError("Hessian instance must be the same")
+        if hasattr(diagonal, "copy_device_to_host"):
+            diagonal.copy_device_to_host()
+        if hasattr(self.hessian, "copy_data_device_to_host"):
+            self.hessian.copy_data_device_to_host()
+        self._dev = self.ldl.device_values(diagonal)
+
+    def factor_perturbed(self, delta_x, delta_c):
+        """One attempt on the loaded system; returns (npos, nneg)."""
+        vals, diag = self._dev
+        return self.ldl.factor_perturbed(delta_x, delta_c, vals, diag)

@@ -288,6 +288,67 @@ class SparseLDL:
         _native.check(self._h, st, "value_gradient")
         return gvals, gdiag
 
+    # -- inertia correction -----------------------------------------------------
+    def set_perturbation_rows(self, primal, dual):
+        """Rows that take +delta_x (primal) and -delta_c (constraints) in
+        :meth:`factor_perturbed`: the index sets of
+        problem.get_primal_indices / get_constraint_indices
+        (amigo/algorithm/solvers/inertia_correction.py:280-293)."""
+        p = np.ascontiguousarray(np.asarray(primal).ravel(), dtype=np.int32)
+        d = np.ascontiguousarray(np.asarray(dual).ravel(), dtype=np.int32)
+        st = self._lib.b200ldl_set_perturbation_rows(
+            self._h, len(p), p.ctypes.data_as(_native._i32p), len(d),
+            d.ctypes.data_as(_native._i32p))
+        _native.check(self._h, st, "set_perturbation_rows")
+
+    def device_values(self, diagonal=None):
+        """The CSR values and the diagonal as float64 CUDA tensors (uploaded
+        when they are host arrays), for repeated :meth:`factor_perturbed`
+        attempts on one system."""
+        import torch
+
+        vals = _values_of(self.mat)
+        diag = _values_of(diagonal)
+        dev = vals.device if _is_torch(vals) and vals.is_cuda else torch.device("cuda")
+        v = torch.as_tensor(np.asarray(vals) if not _is_torch(vals) else vals, device=dev)
+        v = v.to(torch.float64).contiguous()
+        d = None
+        if diag is not None:
+            d = torch.as_tensor(np.asarray(diag) if not _is_torch(diag) else diag, device=dev)
+            d = d.to(torch.float64).contiguous()
+        return v, d
+
+    def factor_perturbed(self, delta_x: float, delta_c: float, vals=None, diag=None):
+        """One inertia-correction attempt: factor K + diag(diag + delta_x on
+        the primal rows - delta_c on the constraint rows), the perturbed
+        diagonal formed on the device, and return the inertia (npos, nneg).
+        ``vals``/``diag`` are CUDA tensors from :meth:`device_values` (by
+        default the matrix's own values and no diagonal)."""
+        if vals is None:
+            vals, diag = self.device_values(diag)
+        self._keep = [vals, diag]
+        self._sync_stream(vals)
+        p = ctypes.c_int()
+        q = ctypes.c_int()
+        st = self._lib.b200ldl_factor_perturbed(
+            self._h, ctypes.c_void_p(vals.data_ptr()),
+            ctypes.c_void_p(diag.data_ptr()) if diag is not None else None,
+            float(delta_x), float(delta_c), ctypes.byref(p), ctypes.byref(q))
+        _native.check(self._h, st, "factor_perturbed")
+        return p.value, q.value
+
+    def perturbed_diagonal(self):
+        """The diagonal of the last :meth:`factor_perturbed` (a CUDA tensor)."""
+        import torch
+
+        out = torch.empty(self.n, dtype=torch.float64, device="cuda")
+        if self._keep and self._keep[0] is not None:
+            out = out.to(self._keep[0].device)
+            self._sync_stream(out)
+        st = self._lib.b200ldl_copy_perturbed_diagonal(self._h, ctypes.c_void_p(out.data_ptr()))
+        _native.check(self._h, st, "perturbed_diagonal")
+        return out
+
     def get_inertia(self):
         p = ctypes.c_int()
         q = ctypes.c_int()

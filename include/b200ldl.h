@@ -125,6 +125,31 @@ int b200ldl_value_gradient(b200ldl_t h, int nrhs, const double* lam, int ldl, co
 /* Number of systems in the handle (1 for b200ldl_create). */
 int b200ldl_num_systems(b200ldl_t h);
 
+/* Inertia correction, one attempt per call (Algorithm IC of Waechter and
+ * Biegler, as amigo/algorithm/solvers/inertia_correction.py:308-383 drives
+ * it). b200ldl_set_perturbation_rows stores, once per pattern, the rows that
+ * take +delta_x (primal, HOST array of nprimal distinct indices) and those
+ * that take -delta_c (constraints, ndual distinct indices): the index sets
+ * InertiaCorrector._compute_perturbation adds to (lines 280-293, which use
+ * problem.get_primal_indices / get_constraint_indices). */
+int b200ldl_set_perturbation_rows(b200ldl_t h, int nprimal, const int* primal, int ndual,
+                                  const int* dual);
+
+/* Factor K + diag(d) with d = diag (+ delta_x on the primal rows when
+ * delta_x > 0) (- delta_c on the constraint rows when delta_c > 0), formed
+ * on the device in that order (vals, diag DEVICE; diag may be NULL), and
+ * return the inertia (npos, nneg: HOST, may be NULL). Replaces
+ * InertiaCorrector._apply_and_factor (inertia_correction.py:308-316), whose
+ * caller passes delta_x = numerical_eps + delta_w: the values and the
+ * diagonal stay on the device across attempts and only the two counts come
+ * back. delta_x and delta_c must be finite and >= 0. */
+int b200ldl_factor_perturbed(b200ldl_t h, const double* vals, const double* diag,
+                             double delta_x, double delta_c, int* npos, int* nneg);
+
+/* The diagonal d of the last b200ldl_factor_perturbed into out [n] (DEVICE),
+ * e.g. for b200ldl_solve_refine against the matrix that was factored. */
+int b200ldl_copy_perturbed_diagonal(b200ldl_t h, double* out);
+
 /* Inertia of every system of the last factorization (arrays of
  * b200ldl_num_systems entries), with get_inertia's counting rule. */
 int b200ldl_system_inertia(b200ldl_t h, int* npos, int* nneg);
