@@ -42,6 +42,10 @@ struct BcShared {
   ChainXchg<kBcCL, 2> x;
   int piv[NB];  // physical rows of the panel's pivots
   int scan[kBcWarps];
+  double Wm[kChain][NB + 1];           // W(pc_m, :) of the columns being formed
+  int pcs[kChain];                     // their physical columns
+  ColStat red[kBcWarps][kChain];       // per-warp column statistics
+  double red2[kBcWarps][kChain];       // per-warp imax-column maxima
 };
 
 // Shared-memory layout (bytes): the panel's L for own rows [R][NB + 1]
@@ -64,55 +68,84 @@ __device__ __forceinline__ double fsym(const double* F, int f, int a, int b) {
   return (a >= b) ? F[a + (size_t)f * b] : F[b + (size_t)f * a];
 }
 
-// Column pc of the panel's Schur complement on this CTA's rows, by one
-// warp; w holds W(pc, :) (zero beyond the panel's width). kRowsPerLane rows
-// per lane pass so that their HBM loads are in flight together (more rows
-// in flight measured slower: the strided loads of the row part queue up).
-constexpr int kRowsPerLane = 4;
-template <int NB, typename Use>
-__device__ __forceinline__ void big_member_column(const double* F, int f, const double* Lp,
-                                                  const unsigned short* ipos, int r0, int Q,
-                                                  int pc, int k, int kwn, int lane,
-                                                  const double* w, double* out, Use use) {
-  constexpr int kNB = NB;
+// d(8x8) += a(8x4) b(4x8) on the FP64 tensor cores. Fragments: lane l
+// holds a(l / 4, l % 4), b(l % 4, l / 4) and d(l / 4, 2 (l % 4) + {0, 1}).
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// Columns pc_m (m in mask, up to 8) of the panel's Schur complement on this
+// CTA's rows, v(r, m) = F(r, pc_m) - Lp(r, :) W(pc_m, :)^T, by all warps
+// together. Rows go in tiles of 8 over the warps. The product of a tile with
+// the 8 columns is one 8x8 FP64 tensor-core tile per 4 panel columns, so
+// Lp is read once for all the columns. The F entries of a whole sweep of
+// tiles are loaded before the products, so that their latencies overlap.
+// Chunk x of the panel columns holds columns 16 (x / 4) + (x % 4) + 4 j,
+// j = 0..3. With the odd row stride of Lp, the 8x4 A fragment then falls
+// on distinct banks. Columns at and beyond the panel's width are zero in
+// Lp and in Wm; chunks entirely beyond it are skipped (exact). emit(m, q,
+// pos, pc, v) is called for every own row q with position pos >= k.
+constexpr int kSweepTiles = 8;
+template <int NB, typename Emit>
+__device__ __forceinline__ void panel_columns(const double* F, int f, const double* Lp,
+                                              const double* Wm, const int* pcs, unsigned mask,
+                                              const unsigned short* ipos, int r0, int Q, int k,
+                                              int kwn, int warp, int lane, Emit emit) {
   constexpr int kNBP = NB + 1;
-  for (int qb = lane; qb < Q; qb += 32 * kRowsPerLane) {
-    double fv4[kRowsPerLane];
-    int pos4[kRowsPerLane];
+  constexpr int kChunks = NB / 4;
+  const int g = lane >> 2;
+  const int tig = lane & 3;
+  const int m0 = 2 * tig;
+  const int m1 = m0 + 1;
+  const bool h0 = (mask >> m0) & 1u;
+  const bool h1 = (mask >> m1) & 1u;
+  const int pc0 = h0 ? pcs[m0] : 0;
+  const int pc1 = h1 ? pcs[m1] : 0;
+  double bf[kChunks];
 #pragma unroll
-    for (int u = 0; u < kRowsPerLane; u++) {
-      const int q = qb + 32 * u;
-      pos4[u] = -1;
-      fv4[u] = 0.0;
+  for (int x = 0; x < kChunks; x++) bf[x] = Wm[g * kNBP + 16 * (x / 4) + (x % 4) + 4 * tig];
+  const int ntiles = (Q + 7) >> 3;
+  for (int i0 = warp; i0 < ntiles; i0 += kBcWarps * kSweepTiles) {
+    double f0[kSweepTiles], f1[kSweepTiles];
+    int pos[kSweepTiles];
+#pragma unroll
+    for (int u = 0; u < kSweepTiles; u++) {
+      const int q = 8 * (i0 + kBcWarps * u) + g;
+      pos[u] = -1;
+      f0[u] = 0.0;
+      f1[u] = 0.0;
       if (q < Q) {
         const int r = r0 + q;
-        pos4[u] = ipos[r];
-        if (pos4[u] >= k) fv4[u] = fsym(F, f, r, pc);
-      }
-    }
-#pragma unroll
-    for (int u = 0; u < kRowsPerLane; u++) {
-      if (pos4[u] < k) continue;
-      const int q = qb + 32 * u;
-      const double* lr = Lp + (size_t)q * kNBP;
-      double a0 = 0.0, a1 = 0.0;
-      // columns at and beyond the panel's width are zero: skip them in
-      // groups of 8 (exact, the skipped products are zeros)
-#pragma unroll
-      for (int c8 = 0; c8 < kNB; c8 += 8) {
-        if (c8 >= kwn) break;
-#pragma unroll
-        for (int c = c8; c < c8 + 8; c += 2) {
-          a0 = fma(lr[c], w[c], a0);
-          a1 = fma(lr[c + 1], w[c + 1], a1);
+        pos[u] = ipos[r];
+        if (pos[u] >= k) {
+          if (h0) f0[u] = fsym(F, f, r, pc0);
+          if (h1) f1[u] = fsym(F, f, r, pc1);
         }
       }
-      const double v = fv4[u] - (a0 + a1);
-      out[q] = v;
-      use(q, r0 + q, pos4[u], v);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int u = 0; u < kSweepTiles; u++) {
+      const int tile = i0 + kBcWarps * u;
+      if (tile >= ntiles) break;  // the same in every lane
+      // rows of the last tile beyond Q read the next shared array (never used)
+      const double* arow = Lp + (size_t)(8 * tile + g) * kNBP + 4 * tig;
+      double c0 = 0.0, c1 = 0.0;
+#pragma unroll
+      for (int x = 0; x < kChunks; x++) {
+        if (16 * (x / 4) >= kwn) break;  // the same in every lane
+        dmma(c0, c1, arow[16 * (x / 4) + (x % 4)], bf[x]);
+      }
+      if (pos[u] >= k) {
+        const int q = 8 * tile + g;
+        if (h0) emit(m0, q, pos[u], pc0, f0[u] - c0);
+        if (h1) emit(m1, q, pos[u], pc1, f1[u] - c1);
+      }
+      __syncwarp();
     }
   }
-  __syncwarp();
 }
 
 template <int NB>
@@ -182,7 +215,8 @@ __global__ void __launch_bounds__(kBcThreads)
     double* cb1 = cb0 + (size_t)kChain * R;
     const int kw_safe = kw - prev_n;
 
-    // ---- exchange 1: warp t forms the column of chain member t
+    // ---- exchange 1: the chain members' columns. Warp t brings member t's
+    // W row; then all warps form all members' columns over row tiles.
     if (warp < nS) {
       const int t = warp;
       const int pc = (t == 0) ? perm[k] : perm[ncand - t];
@@ -194,14 +228,16 @@ __global__ void __launch_bounds__(kBcThreads)
         const double* src = (lane == kw_safe) ? prevA : prevB;
         wl = at_rank(cl, src, o, rank)[pc - kstart - o * R];
       }
-      double w[kNB];
-#pragma unroll
-      for (int c = 0; c < kNB; c++) w[c] = __shfl_sync(0xffffffffu, wl, c);
-      double bv = 0.0, cm = 0.0;
-      int bi = INT_MAX;
-      double* out = cb0 + (size_t)t * R;
-      big_member_column<NB>(F, f, Lp, ipos, r0, Q, pc, k, kw, lane, w, out,
-                        [&](int q, int r, int pos, double v) {
+      if (lane < kNB) sh.Wm[t][lane] = wl;
+      if (lane == 0) sh.pcs[t] = pc;
+    }
+    __syncthreads();
+    {
+      double bv[2] = {0.0, 0.0}, cm[2] = {0.0, 0.0};
+      int bi[2] = {INT_MAX, INT_MAX};
+      panel_columns<NB>(F, f, Lp, &sh.Wm[0][0], sh.pcs, (1u << nS) - 1u, ipos, r0, Q, k, kw,
+                        warp, lane, [&](int m, int q, int pos, int, double v) {
+                          cb0[(size_t)m * R + q] = v;
                           int j = -1;
                           if (pos == k)
                             j = 0;
@@ -209,13 +245,47 @@ __global__ void __launch_bounds__(kBcThreads)
                             j = ncand - pos;
                           if (j >= 0) {
                             for (int d = 0; d < kBcCL; d++)
-                              *at_rank(cl, &sh.x.V[par][t][j], d, rank) = v;
+                              *at_rank(cl, &sh.x.V[par][m][j], d, rank) = v;
                           } else if (pos < ncand) {
-                            keep_larger(bv, bi, fabs(v), pos);
+                            keep_larger(bv[m & 1], bi[m & 1], fabs(v), pos);
                           } else {
-                            cm = fmax(cm, fabs(v));
+                            cm[m & 1] = fmax(cm[m & 1], fabs(v));
                           }
                         });
+      // the 8 lanes with the same lane % 4 hold the same two members
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+#pragma unroll
+        for (int o = 4; o < 32; o <<= 1) {
+          const double ov = __shfl_xor_sync(0xffffffffu, bv[i], o);
+          const int oi = __shfl_xor_sync(0xffffffffu, bi[i], o);
+          keep_larger(bv[i], bi[i], ov, oi);
+          cm[i] = fmax(cm[i], __shfl_xor_sync(0xffffffffu, cm[i], o));
+        }
+      }
+      if (lane < 4) {
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+          ColStat st;
+          st.bv = bv[i];
+          st.cm = cm[i];
+          st.bi = bi[i];
+          st.pad = 0;
+          sh.red[warp][2 * lane + i] = st;
+        }
+      }
+    }
+    __syncthreads();
+    if (warp < nS) {
+      const int t = warp;
+      double bv = 0.0, cm = 0.0;
+      int bi = INT_MAX;
+      if (lane < kBcWarps) {
+        const ColStat st = sh.red[lane][t];
+        bv = st.bv;
+        cm = st.cm;
+        bi = st.bi;
+      }
       warp_argmax_max(bv, bi, cm);
       if (lane < kBcCL) {
         ColStat st;
@@ -235,32 +305,46 @@ __global__ void __launch_bounds__(kBcThreads)
     int d1l;
     const unsigned need2 = need_rows(sh.x.cand, nS, lane, acc1, d1l);
     if (need2) {
-      // ---- exchange 2: warp t forms the imax column of member t (every W
-      // column is in HBM by now)
+      // ---- exchange 2: the imax columns of the members that need them (every
+      // W column is in HBM by now), formed like the member columns
       if (need2 & (1u << warp)) {
         const int t = warp;
         const int pc = sh.x.cand[t].imaxp;
-        const double wl = (lane < kw) ? __ldcg(Wph + (size_t)lane * f + pc) : 0.0;
-        double w[kNB];
-#pragma unroll
-        for (int c = 0; c < kNB; c++) w[c] = __shfl_sync(0xffffffffu, wl, c);
-        double rm = 0.0;
-        double* out = cb1 + (size_t)t * R;
-        const double* colk = cb0 + (size_t)t * R;
-        big_member_column<NB>(F, f, Lp, ipos, r0, Q, pc, k, kw, lane, w, out,
-                          [&](int q, int r, int pos, double v) {
-                            if (r == pc) {
-                              const double wik = colk[q];
+        if (lane < kNB) sh.Wm[t][lane] = (lane < kw) ? __ldcg(Wph + (size_t)lane * f + pc) : 0.0;
+        if (lane == 0) sh.pcs[t] = pc;
+      }
+      __syncthreads();
+      {
+        double rm[2] = {0.0, 0.0};
+        panel_columns<NB>(F, f, Lp, &sh.Wm[0][0], sh.pcs, need2, ipos, r0, Q, k, kw, warp, lane,
+                          [&](int m, int q, int, int pc, double v) {
+                            cb1[(size_t)m * R + q] = v;
+                            if (r0 + q == pc) {
+                              const double wik = cb0[(size_t)m * R + q];
                               for (int d = 0; d < kBcCL; d++) {
-                                double* dst = at_rank(cl, &sh.x.P2[par][t][0], d, rank);
+                                double* dst = at_rank(cl, &sh.x.P2[par][m][0], d, rank);
                                 dst[0] = v;
                                 dst[1] = wik;
                               }
                             } else {
-                              rm = fmax(rm, fabs(v));
+                              rm[m & 1] = fmax(rm[m & 1], fabs(v));
                             }
                           });
-        rm = warp_max_nonneg(rm);
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+#pragma unroll
+          for (int o = 4; o < 32; o <<= 1)
+            rm[i] = fmax(rm[i], __shfl_xor_sync(0xffffffffu, rm[i], o));
+        }
+        if (lane < 4) {
+          sh.red2[warp][2 * lane] = rm[0];
+          sh.red2[warp][2 * lane + 1] = rm[1];
+        }
+      }
+      __syncthreads();
+      if (need2 & (1u << warp)) {
+        const int t = warp;
+        const double rm = warp_max_nonneg((lane < kBcWarps) ? sh.red2[lane][t] : 0.0);
         if (lane < kBcCL) *at_rank(cl, &sh.x.s2[par][rank][t], lane, rank) = rm;
       }
       cl.sync();  // B2
