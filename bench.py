@@ -332,6 +332,13 @@ def run_ours(args, world, rank, local):
         "solve_forward": ("hbm", stats["L_bytes"]),
         "solve_backward": ("hbm", stats["L_bytes"]),
     }
+    # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum,
+    # averaged over every launch of the class's kernel in one factorization
+    # and solve) from the ncu launch list of this workload, kept in
+    # profiles/launch_list_plane_stress_256.txt
+    ncu_traffic = {"big_panel": 2.833e6, "cluster_fronts": 19.887e6, "big_update": 33.788e6,
+                   "fronts": 5.737e6} if (args.workload == "plane_stress"
+                                          and args.nel == 256) else {}
     for p_ in prof or []:
         p_["bound"], w = algo[p_["name"]]
         p_["work_per_step"] = w
@@ -344,14 +351,16 @@ def run_ours(args, world, rank, local):
     elif dom["bound"] == "hbm":
         achieved = total_work / max(1e-12, dom["ms"] / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                "frac": achieved / peaks["hbm_gbs"], "traffic": ncu_traffic.get(dom["name"]),
+                "traffic_unit": "bytes per launch (ncu)",
                 "kernel": dom["name"], "launches": dom["launches"],
                 "ms_per_launch": per_launch_ms, "peak_source": peaks["source"],
                 "timing": "profile pass of the same steps, CUDA events per kernel class"}
     else:
         achieved = total_work / max(1e-12, dom["ms"] / 1e3) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"],
-                "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"], "traffic": None,
+                "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"],
+                "traffic": ncu_traffic.get(dom["name"]), "traffic_unit": "bytes per launch (ncu)",
                 "kernel": dom["name"], "launches": dom["launches"],
                 "ms_per_launch": per_launch_ms, "peak_source": peaks["source"],
                 "note": "FP64 arithmetic measured against the bf16 dense peak; the chained "
