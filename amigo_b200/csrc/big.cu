@@ -650,13 +650,35 @@ __global__ void __launch_bounds__(kUpdThreads, 2)
       }
     }
     __syncthreads();
-    for (int q = tid; q < kw * kTile; q += blockDim.x) {
-      const int c = q / kTile;
-      const int r = q - c * kTile;
-      const int i = i0 + r;
-      const int j = j0 + r;
-      As[c][r] = (i < f) ? F0[i + (size_t)f * (ks + c)] : 0.0;
-      Bs[c][r] = (j < f) ? W[(size_t)c * f + j] : 0.0;
+    {
+      // the panel's rows of L and W for this tile: every load of the thread
+      // is issued before the first shared-memory store, so that the tile
+      // waits on HBM once rather than once per column
+      constexpr int kPer = kBigPanelMax * kTile / kUpdThreads;
+      static_assert(kPer * kUpdThreads == kBigPanelMax * kTile, "panel split");
+      double pa[kPer], pb[kPer];
+#pragma unroll
+      for (int u = 0; u < kPer; u++) {
+        const int q = tid + kUpdThreads * u;
+        const int c = q / kTile;
+        const int r = q - c * kTile;
+        pa[u] = 0.0;
+        pb[u] = 0.0;
+        if (c < kw) {
+          if (i0 + r < f) pa[u] = F0[i0 + r + (size_t)f * (ks + c)];
+          if (j0 + r < f) pb[u] = W[(size_t)c * f + j0 + r];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kPer; u++) {
+        const int q = tid + kUpdThreads * u;
+        const int c = q / kTile;
+        const int r = q - c * kTile;
+        if (c < kw) {
+          As[c][r] = pa[u];
+          Bs[c][r] = pb[u];
+        }
+      }
     }
     __syncthreads();
     double acc[4][4];
