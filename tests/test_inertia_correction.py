@@ -73,3 +73,23 @@ def test_fixture_covers_every_branch(ref_runs):
     assert len(jac[3]["attempts"]) == 1 and jac[3]["attempts"][0][1] > 0  # pre-applied
     hess = ref_runs["hessian_degenerate"]
     assert len(hess[3]["attempts"]) == 1 and hess[3]["attempts"][0][0] > 0
+
+
+def test_perturbation_entry_points_reject_bad_arguments():
+    """Host-side checks of the C ABI, made before any device work."""
+    from amigo_b200 import _native
+    from amigo_b200.sparse_ldl import CSRMat, SparseLDL
+    from amigo_b200.workloads import poisson_2d
+
+    rowp, cols, vals = poisson_2d(5)
+    n = len(rowp) - 1
+    ldl = SparseLDL(CSRMat(n, n, rowp, cols, vals))
+    for primal, dual, why in (([0, n], [1], "out of range"), ([0, 0], [1], "twice"),
+                              ([0], [-1], "out of range"), ([0], [2, 2], "twice")):
+        with pytest.raises(_native.NativeError, match=why):
+            ldl.set_perturbation_rows(primal, dual)
+    lib = _native.load()
+    st = lib.b200ldl_factor_perturbed(ldl._h, None, None, 0.0, 0.0, None, None)
+    assert st < 0 and b"vals is null" in lib.b200ldl_last_error(ldl._h)
+    st = lib.b200ldl_copy_perturbed_diagonal(ldl._h, None)
+    assert st < 0
