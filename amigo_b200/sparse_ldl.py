@@ -21,7 +21,8 @@ import numpy as np
 
 from . import _native
 
-__all__ = ["SolverType", "OrderingType", "CSRMat", "Vector", "SparseLDL", "SparseLDLBatch"]
+__all__ = ["SolverType", "OrderingType", "CSRMat", "Vector", "SparseLDL", "SparseLDLBatch",
+           "SparseCholesky"]
 
 
 class SolverType(enum.IntEnum):
@@ -424,6 +425,47 @@ class SparseLDL:
         _native.check(self._h, st, "stats")
         return {"flops": v[0], "L_bytes": v[1], "cb_bytes": v[2], "max_front": int(v[3]),
                 "delayed": int(v[4]), "levels": int(v[5])}
+
+
+class SparseCholesky:
+    """The reference's SparseCholesky interface (include/sparse_cholesky.h:
+    64-375, bound at amigo/amigo.cpp:641-646) on the GPU factorization.
+
+    The reference factors a symmetric quasi-definite matrix
+    [[A, B^T], [B, -C]] (A, C positive definite; the first ``sqdef_index``
+    rows are A's) in natural order as L L^T over A and -F F^T over the
+    Schur complement of C. A quasi-definite matrix has an LDL^T
+    factorization with 1x1 pivots under every symmetric permutation, so
+    here the threshold test is off (static pivoting: ustab = 0, no delayed
+    pivots) and the rows are ordered by AMD for less fill. The solution is
+    the same; the factor differs from the reference's only by that
+    ordering and the scaling of L by sqrt|D|.
+
+    ``factor()`` returns 0, or 1 when the signs of the pivots do not match
+    the quasi-definite structure (the reference returns the failing
+    Cholesky factorization's flag there). ``solve(x)`` overwrites x with
+    K^{-1} x.
+    """
+
+    def __init__(self, mat, sqdef_index: int | None = None, order=OrderingType.AMD,
+                 pivot_tol: float = 1e-14):
+        if sqdef_index is None and hasattr(mat, "get_sqdef_index"):
+            sqdef_index = mat.get_sqdef_index()
+        self.ldl = SparseLDL(mat, SolverType.LDL, ustab=0.0, pivot_tol=pivot_tol, order=order)
+        n = self.ldl.n
+        self.sqdef_index = n if sqdef_index is None or not 0 <= sqdef_index <= n \
+            else int(sqdef_index)
+
+    def factor(self) -> int:
+        self.ldl.factor(None)
+        npos, nneg = self.ldl.get_inertia()
+        return 0 if (npos, nneg) == (self.sqdef_index, self.ldl.n - self.sqdef_index) else 1
+
+    def solve(self, x):
+        self.ldl.solve(x)
+
+    def get_inertia(self):
+        return self.ldl.get_inertia()
 
 
 class SparseLDLBatch(SparseLDL):

@@ -54,6 +54,11 @@ def load(openmp: bool = False) -> ctypes.CDLL:
     lib.oref_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, _f64p, ctypes.c_int]
     lib.oref_inertia.argtypes = [ctypes.c_void_p, _i32p, _i32p]
     lib.oref_node_pivots.argtypes = [ctypes.c_void_p, _i32p, _i32p]
+    lib.oref_chol_create.restype = ctypes.c_void_p
+    lib.oref_chol_create.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, ctypes.c_int]
+    lib.oref_chol_destroy.argtypes = [ctypes.c_void_p]
+    lib.oref_chol_factor.argtypes = [ctypes.c_void_p, _f64p]
+    lib.oref_chol_solve.argtypes = [ctypes.c_void_p, _f64p]
     _LIBS[key] = lib
     return lib
 
@@ -157,3 +162,41 @@ class RefLDL:
         ndel = np.empty(nn, np.int32)
         self._lib.oref_node_pivots(self._h, _ip(npiv), _ip(ndel))
         return npiv, ndel
+
+
+class RefCholesky:
+    """The reference's SparseCholesky (include/sparse_cholesky.h:64-375):
+    a symmetric quasi-definite matrix factored in natural order, the first
+    ``sqdef_index`` rows forming the positive definite block (-1: all)."""
+
+    def __init__(self, rowp, cols, sqdef_index: int = -1, openmp: bool = False):
+        self._lib = load(openmp)
+        self.rowp = np.ascontiguousarray(rowp, dtype=np.int32)
+        self.cols = np.ascontiguousarray(cols, dtype=np.int32)
+        self.n = len(self.rowp) - 1
+        self._h = self._lib.oref_chol_create(self.n, int(self.rowp[-1]), _ip(self.rowp),
+                                             _ip(self.cols), int(sqdef_index))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.oref_chol_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def factor(self, vals) -> int:
+        vals = np.ascontiguousarray(vals, dtype=np.float64)
+        return self._lib.oref_chol_factor(self._h, _fp(vals))
+
+    def solve(self, b: np.ndarray) -> np.ndarray:
+        """K^{-1} b for one right-hand side (1-D) or each column of a 2-D b."""
+        b = np.asarray(b, dtype=np.float64)
+        if b.ndim == 1:
+            x = np.array(b, copy=True)
+            self._lib.oref_chol_solve(self._h, _fp(x))
+            return x
+        return np.stack([self.solve(b[:, j]) for j in range(b.shape[1])], axis=1)

@@ -31,6 +31,7 @@
 #include <vector>
 
 #define private public
+#include "sparse_cholesky.h"
 #include "sparse_ldl.h"
 #undef private
 
@@ -189,6 +190,48 @@ void oref_node_pivots(void* p, int* num_pivots, int* num_delayed) {
     if (num_pivots) num_pivots[ks] = np;
     if (num_delayed) num_delayed[ks] = nd;
   }
+}
+
+/* The reference's SparseCholesky (include/sparse_cholesky.h): the
+ * factorization of a symmetric quasi-definite matrix in natural order, the
+ * first sqdef_index rows the positive definite block (sqdef_index < 0 or
+ * > n: the whole matrix). */
+struct RefChol {
+  int n = 0;
+  int nnz = 0;
+  std::vector<int> rowp, cols;
+  std::shared_ptr<CSRMat<double>> mat;
+  std::unique_ptr<amigo::SparseCholesky<double>> chol;
+};
+
+void* oref_chol_create(int n, int nnz, const int* rowp, const int* cols, int sqdef_index) {
+  auto* h = new RefChol;
+  h->n = n;
+  h->nnz = nnz;
+  h->rowp.assign(rowp, rowp + n + 1);
+  h->cols.assign(cols, cols + nnz);
+  h->mat = CSRMat<double>::create_from_csr_data(n, n, nnz, h->rowp.data(), h->cols.data(),
+                                                MemoryLocation::HOST_ONLY, nullptr, nullptr,
+                                                sqdef_index);
+  h->chol = std::make_unique<amigo::SparseCholesky<double>>(h->mat);
+  return h;
+}
+
+void oref_chol_destroy(void* p) { delete static_cast<RefChol*>(p); }
+
+int oref_chol_factor(void* p, const double* data) {
+  auto* h = static_cast<RefChol*>(p);
+  std::copy(data, data + h->nnz, h->mat->get_data_ptr());
+  return h->chol->factor();
+}
+
+/* x (n) is overwritten with K^{-1} x. */
+void oref_chol_solve(void* p, double* x) {
+  auto* h = static_cast<RefChol*>(p);
+  Vector<double> v(h->n, 0, MemoryLocation::HOST_ONLY);
+  std::copy(x, x + h->n, v.get_array());
+  h->chol->solve(&v);
+  std::copy(v.get_array(), v.get_array() + h->n, x);
 }
 
 }  // extern "C"

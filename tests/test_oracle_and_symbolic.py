@@ -123,3 +123,17 @@ def test_poisson_generator_matches_reference_matrix(golden):
         g[np.repeat(np.arange(m), np.diff(gr)), golden[f"poisson{n}/cols"]] = \
             golden[f"poisson{n}/vals"]
         assert np.array_equal(a, g)
+
+
+def test_reference_cholesky_oracle_on_golden_cases(golden):
+    """The compiled reference SparseCholesky solves the golden positive
+    definite cases and refuses the indefinite ones."""
+    for name in golden["names"]:
+        rowp, cols, vals = (golden[f"{name}/{k}"] for k in ("rowp", "cols", "vals"))
+        c = ref.RefCholesky(rowp, cols)
+        flag = c.factor(vals)
+        spd = tuple(golden[f"{name}/natural/inertia"])[1] == 0
+        assert (flag == 0) == spd, name
+        if spd:
+            x = c.solve(golden[f"{name}/rhs"])
+            assert np.abs(x - golden[f"{name}/x"]).max() < 1e-11, name
