@@ -436,8 +436,9 @@ class SparseCholesky:
     rows are A's) in natural order as L L^T over A and -F F^T over the
     Schur complement of C. A quasi-definite matrix has an LDL^T
     factorization with 1x1 pivots under every symmetric permutation, so
-    here the threshold test is off (static pivoting: ustab = 0, no delayed
-    pivots) and the rows are ordered by AMD for less fill. The solution is
+    here the threshold test is off (ustab = 0: every pivot is accepted where
+    it stands, so nothing is delayed; fronts without contribution rows keep
+    Bunch-Kaufman) and the rows are ordered by AMD for less fill. The solution is
     the same; the factor differs from the reference's only by that
     ordering and the scaling of L by sqrt|D|.
 
