@@ -415,15 +415,27 @@ def run_batched(args, world, rank, local):
     """Secondary workload: many independent optimal-control KKT systems of
     uneven size (N ~ U{50..400}, nx = 6, nu = 3, one RHS each), factored and
     solved together in one handle. One step = factor + solve of all systems.
-    Not the headline metric; printed in the same JSON shape."""
+    With N ranks the batch is split by system over the GPUs (balanced by
+    size, amigo_b200.shard), no exchange on the data path, and the step time
+    is the slowest rank's (strong scaling of one batch). Not the headline
+    metric; printed in the same JSON shape."""
     import torch
 
+    from amigo_b200.shard import gather_by_system, shard_systems
     from amigo_b200.sparse_ldl import CSRMat, OrderingType, SparseLDLBatch, Vector
     from amigo_b200.workloads import batched_optimal_control
 
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
-    systems = batched_optimal_control(num_systems=args.systems, seed=0)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+    all_systems = batched_optimal_control(num_systems=args.systems, seed=0)
+    idx, systems = shard_systems(all_systems, rank, world)
     mats = [CSRMat(q.n, q.n, q.rowp, q.cols, torch.as_tensor(q.vals, device=dev))
             for q in systems]
     batch = SparseLDLBatch(mats, order=OrderingType.AMD)
@@ -440,6 +452,9 @@ def run_batched(args, world, rank, local):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
     stream = torch.cuda.current_stream(dev)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -449,21 +464,33 @@ def run_batched(args, world, rank, local):
         step()
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        torch.distributed.barrier()
+    t = torch.tensor([e0.elapsed_time(e1) / args.steps], device=dev, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms = float(t.item())
     launches = batch.launch_count() - launches0
     xh = x.cpu().numpy()
-    berr = max(backward_error(q, xs.reshape(-1, 1), q.rhs[:, :1])
-               for q, xs in zip(systems, batch.split(xh)))
-    inertia = batch.system_inertia()
-    ok = all(tuple(i) == q.expected_inertia for i, q in zip(inertia, systems))
+    berrs = [backward_error(q, xs.reshape(-1, 1), q.rhs[:, :1])
+             for q, xs in zip(systems, batch.split(xh))]
+    inertias = [tuple(int(v) for v in i) for i in batch.system_inertia()]
+    # per-system results of every rank, in the batch's order (host gather)
+    results = gather_by_system(list(zip(inertias, berrs)), idx, len(all_systems))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return 0
+    berr = max(r[1] for r in results)
+    ok = all(r[0] == q.expected_inertia for r, q in zip(results, all_systems))
     cpu = None
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:
         from oracle import ref
 
         if ref.available():
             # serial reference, one system after another, on a bounded sample
             t_all, done, n_done = time.perf_counter(), 0.0, 0
-            for q in systems:
+            for q in all_systems:
                 r = ref.RefLDL(q.rowp, q.cols, order=ref.ORDER_AMD)
                 t0 = time.perf_counter()
                 r.factor(q.vals, q.diag)
@@ -473,18 +500,21 @@ def run_batched(args, world, rank, local):
                 n_done += 1
                 if time.perf_counter() - t_all > 20.0:
                     break
-            per_batch = done / n_done * len(systems)
+            per_batch = done / n_done * len(all_systems)
             cpu = {"value": 1.0 / per_batch, "unit": "batch factor+solve/s", "cores": 1,
                    "kind": "reference",
-                   "sample": f"{n_done} of {len(systems)} systems, serial, scaled to the batch"}
+                   "sample": f"{n_done} of {len(all_systems)} systems, serial, scaled to the batch"}
+    n_total = sum(q.n for q in all_systems)
     line = {
-        "metric": METRIC, "value": 1e3 / ms, "unit": "batch factor+solve/s", "n_gpus": 1,
+        "metric": METRIC, "value": 1e3 / ms, "unit": "batch factor+solve/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
-        "config": {"workload": f"{len(systems)} independent optimal-control KKT systems "
-                               f"(n total {batch.n}), one RHS each, AMD, FP64, one handle",
-                   "systems_per_s": len(systems) * 1e3 / ms},
+        "higher_is_better": True, "scaling": "strong" if world > 1 else "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{len(all_systems)} independent optimal-control KKT systems "
+                               f"(n total {n_total}), one RHS each, AMD, FP64",
+                   "parallelism": f"systems split over {world} GPUs" if world > 1
+                   else "single GPU, one handle",
+                   "systems_per_s": len(all_systems) * 1e3 / ms},
         "cpu_baseline": cpu, "gpu_launches": launches, "backward_error": berr,
         "berr_target_met": bool(berr <= BERR_TARGET), "inertia_all_expected": ok,
     }
