@@ -194,6 +194,82 @@ def run_reference(args, world, rank):
     return 0
 
 
+def run_reference_batched(args, world, rank):
+    """The reference arm of the batched workload: one serial SparseLDL per
+    system, the systems spread over all host cores by a thread pool (the
+    compiled reference releases the interpreter lock while it factors).
+    Each step factors and solves a bounded sample of the batch, the time
+    scaled to the whole batch."""
+    if rank != 0:
+        return 0
+    from concurrent.futures import ThreadPoolExecutor
+
+    from amigo_b200.workloads import batched_optimal_control
+    from oracle import ref
+
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/liboracle_ref.so not built"}))
+        return 0
+    # one thread per system: BLAS inside each call stays single-threaded
+    # (read when the library is first loaded in this process)
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    os.environ["OMP_NUM_THREADS"] = "1"
+    systems = batched_optimal_control(num_systems=args.systems, seed=0)
+    cores = os.cpu_count() or 1
+    handles = [ref.RefLDL(q.rowp, q.cols, order=ref.ORDER_AMD) for q in systems]
+
+    def one(i):
+        q = systems[i]
+        handles[i].factor(q.vals, q.diag)
+        return i, handles[i].solve(q.rhs[:, :1]), handles[i].inertia()
+
+    budget = float(os.environ.get("REFERENCE_BUDGET_S", "60"))
+    per_step = max(1, budget / max(1, args.steps + 1))
+    times, results = [], {}
+    with ThreadPoolExecutor(max_workers=cores) as pool:
+        for step in range(args.steps + 1):  # the first pass is the warm-up
+            t0 = time.perf_counter()
+            done = 0
+            futs = [pool.submit(one, i) for i in range(len(systems))]
+            for f in futs:
+                i, x, inertia = f.result()
+                results[i] = (x, inertia)
+                done += 1
+                if time.perf_counter() - t0 > per_step:
+                    break
+            for f in futs:
+                f.cancel()
+            while any(not f.done() for f in futs):
+                time.sleep(0.001)
+            if step > 0:
+                times.append((time.perf_counter() - t0) / done * len(systems))
+    ms = 1e3 * float(np.mean(times))
+    value = 1e3 / ms
+    berr = max(backward_error(systems[i], x, systems[i].rhs[:, :1])
+               for i, (x, _) in results.items())
+    ok = all(tuple(inertia) == systems[i].expected_inertia
+             for i, (_, inertia) in results.items())
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "batch factor+solve/s",
+        "n_gpus": world, "steps": len(times), "warmup": 1, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"{len(systems)} independent optimal-control KKT systems, "
+                               "one RHS each, AMD, FP64",
+                   "parallelism": f"one system per host thread, {cores} threads"},
+        "cpu_baseline": {"value": value, "unit": "batch factor+solve/s", "cores": cores,
+                         "kind": "reference",
+                         "sample": f"systems completed within {per_step:.0f} s per step, "
+                                   "scaled to the batch"},
+        "e2e": {"value": value, "unit": "batch factor+solve/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "backward_error": berr, "inertia_all_expected": ok,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -540,6 +616,8 @@ def main(argv=None) -> int:
     args = ap.parse_args(argv)
     world, rank, local = dist_setup()
     if args.workload == "batched":
+        if args.impl == "reference":
+            return run_reference_batched(args, world, rank)
         return run_batched(args, world, rank, local)
     if args.impl == "reference":
         return run_reference(args, world, rank)
