@@ -56,6 +56,15 @@ SIGNATURES = {
     "b200ldl_factor_perturbed": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_double,
                                                 ctypes.c_double, _i32p, _i32p]),
     "b200ldl_copy_perturbed_diagonal": (ctypes.c_int, [_vp, _vp]),
+    "b200ldl_assembly_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, _i32p, _i32p,
+                                               ctypes.c_int, _i32p, _i32p, _i32p]),
+    "b200ldl_assembly_values": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
+    "b200ldl_assembly_info": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong),
+                                             ctypes.c_int]),
+    "b200ldl_assembly_plan": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_longlong),
+                                             ctypes.POINTER(ctypes.c_longlong)]),
+    "b200ldl_assembly_last_error": (ctypes.c_char_p, [_vp]),
+    "b200ldl_assembly_destroy": (None, [_vp]),
 }
 
 

@@ -202,6 +202,48 @@ long long b200ldl_launch_count(b200ldl_t h);
  * fronts factored on chip in a thread-block cluster. */
 int b200ldl_work(b200ldl_t h, double* out, int n);
 
+/* KKT assembly: element Hessian blocks into the values of the fixed CSR
+ * pattern, on the device. Replaces the Hessian assembly of
+ * OptimizationProblem::hessian (include/optimization_problem.h:1063-1088):
+ * the matrix zeroed, then for each component group, element and column j of
+ * the element's Hessian, the column added into CSR row conn[e][j] at
+ * columns conn[e][i] with entries outside the pattern dropped
+ * (ComponentGroup::add_hessian_kernel, include/component_group.h:144-162,
+ * CSRMat::add_row, include/csr_matrix.h:554-567; the GPU backend's
+ * atomicAdd scatter, include/cuda/component_group_backend.cuh:157-190).
+ * The values are summed in exactly that order, so they are bit-identical to
+ * the reference's CPU assembly. */
+typedef struct b200ldl_assembly* b200ldl_assembly_t;
+
+/* Plan the assembly on the host (no device work until the first
+ * b200ldl_assembly_values). rowp/cols: the CSR pattern (n rows, sorted
+ * columns), HOST. ngroups component groups; group g has nelems[g] elements
+ * of ncomp[g] variables; conn: the groups' [nelems][ncomp] global variable
+ * indices one after another (int32, HOST). On failure *out still holds a
+ * handle whose b200ldl_assembly_last_error says why; destroy it. */
+int b200ldl_assembly_create(b200ldl_assembly_t* out, int n, const int* rowp, const int* cols,
+                            int ngroups, const int* nelems, const int* ncomp, const int* conn);
+
+/* vals[nnz] = the assembled CSR values from blocks, the groups' element
+ * blocks one after another, block[e][j][i] = column j, row i of element e's
+ * Hessian (DEVICE pointers; asynchronous on stream, a cudaStream_t or NULL).
+ * The output feeds b200ldl_factor directly. */
+int b200ldl_assembly_values(b200ldl_assembly_t a, const double* blocks, double* vals,
+                            void* stream);
+
+/* out[0] = contributions kept, out[1] = contributions outside the pattern
+ * (dropped, as add_row drops them), out[2] = block values expected,
+ * out[3] = nnz; the first nout of them. */
+int b200ldl_assembly_info(b200ldl_assembly_t a, long long* out, int nout);
+
+/* The plan (HOST arrays, may be NULL): ptr [nnz + 1] and src [out[0] of
+ * b200ldl_assembly_info]; CSR entry p sums blocks[src[ptr[p] .. ptr[p+1])]
+ * in that order. */
+int b200ldl_assembly_plan(b200ldl_assembly_t a, long long* ptr, long long* src);
+
+const char* b200ldl_assembly_last_error(b200ldl_assembly_t a);
+void b200ldl_assembly_destroy(b200ldl_assembly_t a);
+
 /* Allocation-free dense solve (no counterpart in the reference; the
  * reference always allocates its factor storage). For callers that must not
  * allocate device memory while running, e.g. a real-time loop re-solving a

@@ -54,6 +54,8 @@ def load(openmp: bool = False) -> ctypes.CDLL:
     lib.oref_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, _f64p, ctypes.c_int]
     lib.oref_inertia.argtypes = [ctypes.c_void_p, _i32p, _i32p]
     lib.oref_node_pivots.argtypes = [ctypes.c_void_p, _i32p, _i32p]
+    lib.oref_csr_assemble.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, ctypes.c_int,
+                                      _i32p, _i32p, _i32p, _f64p, _f64p]
     lib.oref_chol_create.restype = ctypes.c_void_p
     lib.oref_chol_create.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _i32p, ctypes.c_int]
     lib.oref_chol_destroy.argtypes = [ctypes.c_void_p]
@@ -200,3 +202,25 @@ class RefCholesky:
             self._lib.oref_chol_solve(self._h, _fp(x))
             return x
         return np.stack([self.solve(b[:, j]) for j in range(b.shape[1])], axis=1)
+
+
+def csr_assemble(rowp, cols, groups, blocks) -> np.ndarray:
+    """The reference's Hessian assembly (add_row per element column, in
+    order) of the element blocks into the CSR values. groups: list of
+    [nelem, ncomp] int arrays of global indices; blocks: list of
+    [nelem, ncomp, ncomp] arrays, block[e, j, i] = column j, row i."""
+    lib = load()
+    rowp = np.ascontiguousarray(rowp, dtype=np.int32)
+    cols = np.ascontiguousarray(cols, dtype=np.int32)
+    n = len(rowp) - 1
+    nelems = np.array([g.shape[0] for g in groups], dtype=np.int32)
+    ncomp = np.array([g.shape[1] for g in groups], dtype=np.int32)
+    conn = np.ascontiguousarray(np.concatenate([np.asarray(g, np.int32).ravel() for g in groups])
+                                if groups else np.zeros(1, np.int32), dtype=np.int32)
+    vals = np.ascontiguousarray(np.concatenate([np.asarray(b, np.float64).ravel()
+                                                for b in blocks]) if blocks
+                                else np.zeros(1), dtype=np.float64)
+    out = np.zeros(int(rowp[-1]), dtype=np.float64)
+    lib.oref_csr_assemble(n, int(rowp[-1]), _ip(rowp), _ip(cols), len(groups), _ip(nelems),
+                          _ip(ncomp), _ip(conn), _fp(vals), _fp(out))
+    return out

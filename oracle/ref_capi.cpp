@@ -192,6 +192,31 @@ void oref_node_pivots(void* p, int* num_pivots, int* num_delayed) {
   }
 }
 
+/* The reference's Hessian assembly on one rank: the CSR values zeroed, then
+ * for each group, element and column j of the element's Hessian, CSRMat::
+ * add_row (include/csr_matrix.h:554-567) of that column into row
+ * conn[e][j] at the element's columns, the loop of ComponentGroup::
+ * add_hessian_kernel (include/component_group.h:144-162) with the local and
+ * global indices equal. blocks: the groups' [nelems][ncomp][ncomp] values,
+ * block[e][j][i] = column j, row i. out: nnz values. */
+void oref_csr_assemble(int n, int nnz, const int* rowp, const int* cols, int ngroups,
+                       const int* nelems, const int* ncomp, const int* conn,
+                       const double* blocks, double* out) {
+  std::vector<int> rp(rowp, rowp + n + 1), cl(cols, cols + nnz);
+  auto mat = CSRMat<double>::create_from_csr_data(n, n, nnz, rp.data(), cl.data(),
+                                                  MemoryLocation::HOST_ONLY);
+  mat->zero();
+  const int* c = conn;
+  const double* b = blocks;
+  for (int g = 0; g < ngroups; g++) {
+    const int m = ncomp[g];
+    for (int e = 0; e < nelems[g]; e++, c += m) {
+      for (int j = 0; j < m; j++, b += m) mat->add_row(c[j], m, c, b);
+    }
+  }
+  std::copy(mat->get_data_ptr(), mat->get_data_ptr() + nnz, out);
+}
+
 /* The reference's SparseCholesky (include/sparse_cholesky.h): the
  * factorization of a symmetric quasi-definite matrix in natural order, the
  * first sqdef_index rows the positive definite block (sqdef_index < 0 or
