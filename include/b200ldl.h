@@ -226,7 +226,9 @@ int b200ldl_assembly_create(b200ldl_assembly_t* out, int n, const int* rowp, con
 
 /* vals[nnz] = the assembled CSR values from blocks, the groups' element
  * blocks one after another, block[e][j][i] = column j, row i of element e's
- * Hessian (DEVICE pointers; asynchronous on stream, a cudaStream_t or NULL).
+ * Hessian, which must hold the number of block values b200ldl_assembly_info
+ * reports in out[2] (DEVICE pointers; asynchronous on stream, a
+ * cudaStream_t or NULL).
  * The output feeds b200ldl_factor directly. The plan is copied to the
  * current device at the first call and used there from then on. */
 int b200ldl_assembly_values(b200ldl_assembly_t a, const double* blocks, double* vals,
