@@ -137,3 +137,38 @@ def test_reference_cholesky_oracle_on_golden_cases(golden):
         if spd:
             x = c.solve(golden[f"{name}/rhs"])
             assert np.abs(x - golden[f"{name}/x"]).max() < 1e-11, name
+
+
+def test_batch_symbolic_is_each_systems_own():
+    """A batch handle's merged forest is every system's own symbolic phase,
+    shifted by the system's variable and supernode offsets (host only)."""
+    from amigo_b200.sparse_ldl import SparseLDLBatch
+
+    systems = batched_optimal_control(num_systems=5, seed=11)
+    mats = [CSRMat(q.n, q.n, q.rowp, q.cols, q.vals) for q in systems]
+    batch = SparseLDLBatch(mats, order=OrderingType.AMD)
+    m = batch.symbolic()
+    voff = noff = 0
+    roots = []
+    for q in systems:
+        one = SparseLDL(CSRMat(q.n, q.n, q.rowp, q.cols, q.vals), order=OrderingType.AMD)
+        s = one.symbolic()
+        nn = len(s["node_ptr"]) - 1
+        assert np.array_equal(m["invperm"][voff:voff + q.n], s["invperm"] + voff)
+        assert np.array_equal(m["node_to_var"][voff:voff + q.n], s["node_to_var"] + voff)
+        assert np.array_equal(m["node_ptr"][noff:noff + nn + 1], s["node_ptr"] + voff)
+        for k in range(nn):
+            a0, a1 = m["contrib_ptr"][noff + k], m["contrib_ptr"][noff + k + 1]
+            b0, b1 = s["contrib_ptr"][k], s["contrib_ptr"][k + 1]
+            assert np.array_equal(m["contrib_rows"][a0:a1], s["contrib_rows"][b0:b1] + voff)
+            c0, c1 = m["children_ptr"][noff + k], m["children_ptr"][noff + k + 1]
+            d0, d1 = s["children_ptr"][k], s["children_ptr"][k + 1]
+            assert np.array_equal(m["children"][c0:c1], s["children"][d0:d1] + noff)
+        r0, r1 = s["children_ptr"][nn], s["children_ptr"][nn + 1]
+        roots.extend((s["children"][r0:r1] + noff).tolist())
+        voff += q.n
+        noff += nn
+    total = len(m["node_ptr"]) - 1
+    assert total == noff
+    # every system's roots, in system order, in the merged roots slot
+    assert m["children"][m["children_ptr"][total]:m["children_ptr"][total + 1]].tolist() == roots
