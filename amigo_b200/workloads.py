@@ -365,6 +365,154 @@ def plane_stress_kkt(
     )
 
 
+def _q1_hex_ke(nu: float = 0.3) -> np.ndarray:
+    """24x24 stiffness of a unit-modulus, unit-cube trilinear (Q1) hex
+    element, 2x2x2 Gauss quadrature. Node order: the bottom face (z = -1)
+    (-1,-1), (1,-1), (1,1), (-1,1), then the top face (z = +1) in the same
+    order; dofs (x, y, z) per node. Strains in Voigt order xx, yy, zz, xy,
+    yz, zx."""
+    lam = nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+    mu = 1.0 / (2.0 * (1.0 + nu))
+    D = np.zeros((6, 6))
+    D[:3, :3] = lam
+    D[np.arange(3), np.arange(3)] += 2.0 * mu
+    D[np.arange(3, 6), np.arange(3, 6)] = mu
+    xn = np.array([-1.0, 1.0, 1.0, -1.0, -1.0, 1.0, 1.0, -1.0])
+    yn = np.array([-1.0, -1.0, 1.0, 1.0, -1.0, -1.0, 1.0, 1.0])
+    zn = np.array([-1.0, -1.0, -1.0, -1.0, 1.0, 1.0, 1.0, 1.0])
+    g = 1.0 / math.sqrt(3.0)
+    ke = np.zeros((24, 24))
+    for xi in (-g, g):
+        for eta in (-g, g):
+            for zeta in (-g, g):
+                # reference-cube derivatives; the unit cube maps with
+                # x = (xi + 1) / 2, so d/dx = 2 d/dxi and det J = 1/8
+                dx = 2.0 * 0.125 * xn * (1 + eta * yn) * (1 + zeta * zn)
+                dy = 2.0 * 0.125 * yn * (1 + xi * xn) * (1 + zeta * zn)
+                dz = 2.0 * 0.125 * zn * (1 + xi * xn) * (1 + eta * yn)
+                Bm = np.zeros((6, 24))
+                Bm[0, 0::3] = dx
+                Bm[1, 1::3] = dy
+                Bm[2, 2::3] = dz
+                Bm[3, 0::3] = dy
+                Bm[3, 1::3] = dx
+                Bm[4, 1::3] = dz
+                Bm[4, 2::3] = dy
+                Bm[5, 2::3] = dx
+                Bm[5, 0::3] = dz
+                ke += 0.125 * (Bm.T @ D @ Bm)
+    return ke
+
+
+def hex_elasticity_kkt(
+    nel: int = 48,
+    seed: int = 0,
+    nrhs_random: int = 4,
+    delta: float = 1e-8,
+    nu: float = 0.3,
+    sigma_range: tuple[float, float] = (1e-6, 1e6),
+) -> KKTSystem:
+    """The 3D counterpart of :func:`plane_stress_kkt` with a dense row (the
+    48^3 hex workload): an nel^3 mesh of unit-cube Q1 hex elements.
+
+    Unknowns, in order: u (3 (nel+1)^3 displacements), rho (nel^3
+    densities), lambda (3 (nel+1)^3 equilibrium multipliers), mu (one volume
+    multiplier). Blocks: lambda-u = K(rho) = sum_e rho_e^3 K_e; lambda-rho:
+    3 rho_e^2 K_e u0_e; mu-rho: the element volumes (1 each), a dense row;
+    rho-rho: 1e-3 I; u-u: 0. The face x = 0 is clamped: a clamped dof d
+    keeps only the (lambda_d, u_d) = 1 coupling. Diagonal vector: 0 on u,
+    Sigma log-uniform on ``sigma_range`` on rho, -delta on lambda and mu.
+    Expected inertia: (number of u and rho, number of lambda and mu). RHS:
+    column 0 a unit load (-1 in z at the centre node of the face x = nel, in
+    the lambda block), then ``nrhs_random`` N(0,1) columns.
+
+    Draw order from ``default_rng(seed)``: rho U[0.3, 1] (nel^3), u0 N(0,1)
+    (3 (nel+1)^3), log(Sigma) (nel^3), random RHS (n, nrhs_random).
+    """
+    rng = np.random.default_rng(seed)
+    nn1 = nel + 1
+    nnode = nn1**3
+    nu_dof = 3 * nnode
+    ne = nel**3
+    off_rho = nu_dof
+    off_lam = nu_dof + ne
+    off_mu = off_lam + nu_dof
+    n = off_mu + 1
+    n_primal = nu_dof + ne
+
+    rho = rng.uniform(0.3, 1.0, size=ne)
+    u0 = rng.standard_normal(nu_dof)
+    sigma = np.exp(rng.uniform(math.log(sigma_range[0]), math.log(sigma_range[1]), size=ne))
+    rhs_r = rng.standard_normal((n, nrhs_random))
+
+    ke = _q1_hex_ke(nu)
+    ex, ey, ez = np.meshgrid(np.arange(nel), np.arange(nel), np.arange(nel), indexing="ij")
+    n0 = (ex + ey * nn1 + ez * nn1 * nn1).ravel()
+    face = np.stack([n0, n0 + 1, n0 + 1 + nn1, n0 + nn1], axis=1)
+    nodes = np.concatenate([face, face + nn1 * nn1], axis=1)  # (ne, 8)
+    edofs = np.empty((ne, 24), dtype=np.int64)
+    for d in range(3):
+        edofs[:, d::3] = 3 * nodes + d
+
+    clamped = np.zeros(nu_dof, dtype=bool)
+    jj, kk = np.meshgrid(np.arange(nn1), np.arange(nn1), indexing="ij")
+    x0 = (jj * nn1 + kk * nn1 * nn1).ravel()  # nodes with x index 0
+    for d in range(3):
+        clamped[3 * x0 + d] = True
+
+    kr = np.broadcast_to(edofs[:, :, None], (ne, 24, 24))
+    kc = np.broadcast_to(edofs[:, None, :], (ne, 24, 24))
+    keep = ~(clamped[kr] | clamped[kc])
+    kv = (rho**3)[:, None, None] * ke[None]
+    rows = [off_lam + kr[keep]]
+    cols = [kc[keep]]
+    vals = [kv[keep]]
+    ge = 3.0 * (rho**2)[:, None] * np.einsum("ab,eb->ea", ke, u0[edofs])
+    gkeep = ~clamped[edofs]
+    rows.append(off_lam + edofs[gkeep])
+    cols.append(np.broadcast_to((off_rho + np.arange(ne))[:, None], (ne, 24))[gkeep])
+    vals.append(ge[gkeep])
+    cd = np.nonzero(clamped)[0]
+    rows.append(off_lam + cd)
+    cols.append(cd)
+    vals.append(np.ones(len(cd)))
+    rr = off_rho + np.arange(ne)
+    rows.append(rr)
+    cols.append(rr)
+    vals.append(np.full(ne, 1e-3))
+    # the volume constraint: sum_e rho_e (unit volumes)
+    rows.append(np.full(ne, off_mu))
+    cols.append(rr)
+    vals.append(np.ones(ne))
+
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    v = np.concatenate(vals)
+    r2, c2, v2 = _sym(r, c, v)
+    rowp, colsx, valsx = csr_from_coo(n, r2, c2, v2)
+
+    diag = np.zeros(n)
+    diag[off_rho:off_lam] = sigma
+    diag[off_lam:] = -delta
+
+    rhs = np.zeros((n, 1 + nrhs_random))
+    mid = nel // 2
+    load_node = nel + mid * nn1 + mid * nn1 * nn1  # face x = nel, centre
+    rhs[off_lam + 3 * load_node + 2, 0] = -1.0
+    rhs[:, 1:] = rhs_r
+    return KKTSystem(
+        n=n,
+        rowp=rowp,
+        cols=colsx,
+        vals=valsx,
+        diag=diag,
+        rhs=np.asfortranarray(rhs),
+        n_primal=n_primal,
+        n_con=nu_dof + 1,
+        name=f"hex_elasticity_{nel}^3",
+    )
+
+
 def poisson_2d(n: int, seed: int = 0):
     """5-point Laplacian on the (n-1)^2 interior grid of [0,1]^2, scaled by
     1/h^2, symmetrically permuted by ``np.random.permutation`` after

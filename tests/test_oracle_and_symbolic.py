@@ -172,3 +172,50 @@ def test_batch_symbolic_is_each_systems_own():
     assert total == noff
     # every system's roots, in system order, in the merged roots slot
     assert m["children"][m["children_ptr"][total]:m["children_ptr"][total + 1]].tolist() == roots
+
+
+def test_hex_element_stiffness_has_the_rigid_modes():
+    from amigo_b200.workloads import _q1_hex_ke
+
+    ke = _q1_hex_ke()
+    assert np.abs(ke - ke.T).max() < 1e-15
+    assert np.linalg.matrix_rank(ke) == 18
+    # node coordinates of the unit cube in the element's node order
+    xyz = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                    [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], dtype=float)
+    for d in range(3):
+        t = np.zeros(24)
+        t[d::3] = 1.0
+        assert np.abs(ke @ t).max() < 1e-14
+    for a, b in ((0, 1), (1, 2), (2, 0)):  # small rotations about each axis
+        w = np.zeros(24)
+        w[a::3] = -xyz[:, b]
+        w[b::3] = xyz[:, a]
+        assert np.abs(ke @ w).max() < 1e-14
+
+
+@pytest.mark.parametrize("order", [OrderingType.AMD, OrderingType.NATURAL])
+def test_symbolic_matches_reference_hex_with_dense_row(order):
+    """The 3D workload with its dense volume-constraint row, at small sizes."""
+    from amigo_b200.workloads import hex_elasticity_kkt
+
+    for nel in (2, 4, 6):
+        s = hex_elasticity_kkt(nel)
+        _compare_symbolic(s.rowp, s.cols, order)
+
+
+def test_hex_workload_has_the_designed_inertia():
+    """The compiled reference factors the 3D workload with the inertia the
+    generator promises (n_primal positive, n_con negative) and a FP64
+    backward error."""
+    from amigo_b200.workloads import hex_elasticity_kkt
+
+    for nel in (3, 5):
+        s = hex_elasticity_kkt(nel)
+        r = ref.RefLDL(s.rowp, s.cols, order=ref.ORDER_AMD)
+        r.factor(s.vals, s.diag)
+        assert tuple(r.inertia()) == s.expected_inertia
+        x = r.solve(s.rhs)
+        berr = np.abs(s.matvec(x) - s.rhs).max() / (
+            s.inf_norm() * np.abs(x).max() + np.abs(s.rhs).max())
+        assert berr < 1e-14
