@@ -43,7 +43,7 @@ def test_reference_unit_cases(golden, order):
         assert np.abs(v.array - golden[f"{name}/x"]).max() < 1e-11, name
 
 
-def _check_system(s, order=OrderingType.AMD, nrhs=None):
+def _check_system(s, order=OrderingType.AMD, nrhs=None, fwd_tol=1e-6):
     g = _gpu(s.rowp, s.cols, order)
     g.mat.vals = s.vals
     assert g.factor(Vector(s.diag)) == 0
@@ -62,7 +62,7 @@ def _check_system(s, order=OrderingType.AMD, nrhs=None):
     # cond * eps, so the forward comparison is a loose sanity bound and the
     # backward error above is the accuracy criterion
     rel = np.abs(x - xr).max() / np.abs(xr).max()
-    assert rel < 1e-6, rel
+    assert rel < fwd_tol, rel
     return g, r
 
 
@@ -173,3 +173,16 @@ def test_sparse_cholesky_matches_reference(golden):
     xr = rc.solve(s.rhs)
     assert backward_error(s, x, s.rhs) <= BERR_TOL
     assert np.abs(x - xr).max() / np.abs(xr).max() < 1e-6
+
+
+@pytest.mark.parametrize("nel", [8, 12])
+def test_hex_elasticity_with_dense_row(nel):
+    # the 3D workload at small sizes: fronts with the dense volume row, up to
+    # ~2200 rows at 12^3 (chained big-front panels). Sigma spans 1e-6..1e6,
+    # so two correct FP64 solvers disagree in the forward error: the
+    # reference and a sparse LU of the same matrix differ by 2.2e-6 (8^3) and
+    # 3.4e-5 (12^3) relative. The forward bound is set above that spread;
+    # inertia and the backward error stay exact requirements.
+    from amigo_b200.workloads import hex_elasticity_kkt
+
+    _check_system(hex_elasticity_kkt(nel), fwd_tol=1e-4)
