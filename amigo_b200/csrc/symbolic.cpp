@@ -8,6 +8,10 @@
 #include "symbolic.h"
 
 #include <algorithm>
+#include <climits>
+#include <cstdint>
+#include <set>
+#include <utility>
 #include <cstdio>
 #include <numeric>
 #include <stdexcept>
@@ -28,6 +32,17 @@ int sort_unique_nonneg(int len, int* a) {
     if (i != j) a[j] = a[i];
   }
   return j;
+}
+
+// element lists up to this length test every pair directly
+constexpr int kMergeScanMax = 48;
+
+// a 64-bit mixing function (splitmix64's finalizer)
+inline uint64_t mix64(uint64_t x) {
+  x += 0x9e3779b97f4a7c15ull;
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+  return x ^ (x >> 31);
 }
 
 // Bucketed degree lists with LIFO buckets and a monotonically non-increasing
@@ -179,6 +194,10 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
   }
 
   DegreeBuckets deg(n, rowp);
+  // supervariable detection on long lists (see the merge step)
+  std::vector<int> lp_pos(n, -1), touched;
+  std::vector<uint64_t> merge_keys;
+  std::set<std::pair<uint64_t, int>> by_key[2];
   int nsv = 0;
   for (int i = 0; i < n; nsv++) {
     const int piv = deg.pick();
@@ -319,22 +338,87 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
       for (int k = rowp[v]; k < rowp[v] + g.elen[v]; k++) elem_deg[cols[k]] = -1;
     }
 
-    // merge indistinguishable variables of Lp into supervariables
-    for (int j = 0; j < len; j++) {
-      const int a = Lp[j];
-      if (a == piv || slen[a] < 0) continue;
-      for (int k = j + 1; k < len; k++) {
-        const int b = Lp[k];
-        if (b == piv || slen[b] < 0) continue;
-        if (g.same_adjacency(a, b)) {
-          slen[a] += slen[b];
-          deg.set(a, deg.degree[a] - slen[b]);
-          slen[b] = -(a + 1);
-          state[b] = -1;
-          g.drop_variable(b);
-          deg.unlink(b);
+    // merge indistinguishable variables of Lp into supervariables: pairs
+    // (Lp[j], Lp[k]), k > j, are tested in order and a match is merged at
+    // once (later tests see the merged graph)
+    auto merge = [&](int a, int b) {
+      slen[a] += slen[b];
+      deg.set(a, deg.degree[a] - slen[b]);
+      slen[b] = -(a + 1);
+      state[b] = -1;
+      g.drop_variable(b);
+      deg.unlink(b);
+    };
+    if (len <= kMergeScanMax) {
+      for (int j = 0; j < len; j++) {
+        const int a = Lp[j];
+        if (a == piv || slen[a] < 0) continue;
+        for (int k = j + 1; k < len; k++) {
+          const int b = Lp[k];
+          if (b == piv || slen[b] < 0) continue;
+          if (g.same_adjacency(a, b)) merge(a, b);
         }
       }
+    } else {
+      // Same tests, same order, without the pairs that cannot match. The
+      // test holds only when the lengths agree and either the rows are
+      // equal, or each row holds the other variable and the rows agree
+      // without them. So with R(v) the sum of a hash over v's row, a match
+      // needs R(a) = R(b) or R(a) + h(a) = R(b) + h(b). Positions are kept
+      // in two ordered sets by those keys; the next candidate after k is a
+      // lookup. A merge changes the rows of the dropped variable's
+      // neighbours, whose keys are then recomputed.
+      merge_keys.assign(2 * len, 0);
+      by_key[0].clear();
+      by_key[1].clear();
+      for (int p = 0; p < len; p++) lp_pos[Lp[p]] = p;
+      auto set_keys = [&](int p) {
+        const int v = Lp[p];
+        uint64_t r = 0;
+        for (int q = rowp[v]; q < rowp[v] + g.alen[v]; q++) r += mix64((uint64_t)cols[q]);
+        const uint64_t shape = ((uint64_t)(uint32_t)g.alen[v] << 32) | (uint32_t)g.elen[v];
+        merge_keys[2 * p] = mix64(r ^ mix64(shape));
+        merge_keys[2 * p + 1] = mix64((r + mix64((uint64_t)v)) ^ mix64(shape));
+        by_key[0].insert({merge_keys[2 * p], p});
+        by_key[1].insert({merge_keys[2 * p + 1], p});
+      };
+      auto erase_keys = [&](int p) {
+        by_key[0].erase({merge_keys[2 * p], p});
+        by_key[1].erase({merge_keys[2 * p + 1], p});
+      };
+      for (int p = 0; p < len; p++)
+        if (Lp[p] != piv && slen[Lp[p]] >= 0) set_keys(p);
+      for (int j = 0; j < len; j++) {
+        const int a = Lp[j];
+        if (a == piv || slen[a] < 0) continue;
+        int k = j;
+        for (;;) {
+          int c = INT_MAX;
+          for (int t = 0; t < 2; t++) {
+            const uint64_t key = merge_keys[2 * j + t];
+            auto it = by_key[t].lower_bound({key, k + 1});
+            if (it != by_key[t].end() && it->first == key) c = std::min(c, it->second);
+          }
+          if (c == INT_MAX) break;
+          k = c;
+          const int b = Lp[k];
+          if (!g.same_adjacency(a, b)) continue;
+          // the neighbours of b in Lp whose rows the drop shortens
+          touched.clear();
+          for (int q = rowp[b] + g.elen[b]; q < rowp[b] + g.alen[b]; q++) {
+            const int w = cols[q];
+            if (w >= 0 && w < n && lp_pos[w] >= 0 && w != piv && slen[w] >= 0 && w != b)
+              touched.push_back(lp_pos[w]);
+          }
+          erase_keys(k);
+          merge(a, b);
+          for (const int p : touched) {
+            erase_keys(p);
+            set_keys(p);
+          }
+        }
+      }
+      for (int p = 0; p < len; p++) lp_pos[Lp[p]] = -1;
     }
     i += slen[piv];
   }
