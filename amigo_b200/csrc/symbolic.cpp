@@ -10,7 +10,6 @@
 #include <algorithm>
 #include <climits>
 #include <cstdint>
-#include <set>
 #include <utility>
 #include <cstdio>
 #include <numeric>
@@ -36,6 +35,13 @@ int sort_unique_nonneg(int len, int* a) {
 
 // element lists up to this length test every pair directly
 constexpr int kMergeScanMax = 48;
+// re-keyed positions looked up linearly before the sorted keys are rebuilt
+constexpr size_t kMergeExtraMax = 64;
+// rows longer than this at the start (a dense row, e.g. a constraint
+// coupled to every design variable) keep their slen sum and row hash up to
+// date instead of rescanning the row at every pivot that touches it
+constexpr int kTrackRow = 256;
+constexpr int kTrackMaxRows = 64;
 
 // a 64-bit mixing function (splitmix64's finalizer)
 inline uint64_t mix64(uint64_t x) {
@@ -194,16 +200,42 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
   }
 
   DegreeBuckets deg(n, rowp);
+  // Long rows: vsum[v] = sum of slen over v's variable part, rhash[v] = sum
+  // of mix64 over v's whole row, kept exact through every change to the row
+  // (prune, new element, variable drop) and to slen (merge).
+  std::vector<char> tracked(n, 0);
+  std::vector<long long> vsum(n, 0);
+  std::vector<uint64_t> rhash(n, 0);
+  std::vector<int> tracked_list;
+  for (int v = 0; v < n; v++)
+    if (g.alen[v] > kTrackRow) tracked_list.push_back(v);
+  // the longest few only: every merge checks each tracked row
+  std::stable_sort(tracked_list.begin(), tracked_list.end(),
+                   [&](int x, int y) { return g.alen[x] > g.alen[y]; });
+  if (tracked_list.size() > (size_t)kTrackMaxRows) tracked_list.resize(kTrackMaxRows);
+  for (const int v : tracked_list) {
+    tracked[v] = 1;
+    for (int q = rowp[v]; q < rowp[v] + g.alen[v]; q++) {
+      vsum[v] += slen[cols[q]];
+      rhash[v] += mix64((uint64_t)cols[q]);
+    }
+  }
+  auto in_vars = [&](int v, int x) {
+    const int* b = cols + rowp[v] + g.elen[v];
+    const int* e = cols + rowp[v] + g.alen[v];
+    return std::binary_search(b, e, x);
+  };
   // supervariable detection on long lists (see the merge step)
   std::vector<int> lp_pos(n, -1), touched;
   std::vector<uint64_t> merge_keys;
-  std::set<std::pair<uint64_t, int>> by_key[2];
+  std::vector<std::pair<uint64_t, int>> by_key[2], extra[2];
   int nsv = 0;
   for (int i = 0; i < n; nsv++) {
     const int piv = deg.pick();
     deg.unlink(piv);
     perm[nsv] = piv;
     state[piv] = 0;
+    tracked[piv] = 0;  // its row becomes the new element's
 
     // Lp = {piv} U adj(piv) U adj(elements of piv)
     int len = 0;
@@ -230,13 +262,30 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
         for (int c = rowp[v]; k < kend && c < rowp[v] + g.elen[v]; c++) {
           while (k < kend && cols[k] < cols[c]) k++;
           if (k < kend && cols[k] == cols[c]) {
+            if (tracked[v]) rhash[v] -= mix64((uint64_t)cols[c]);
             cols[c] = -1;
             removed_e++;
           }
         }
       }
       int removed_v = 0;
-      {
+      if (tracked[v]) {
+        // the same entries by binary search over the (sorted) variable part
+        int* vb = cols + rowp[v] + g.elen[v];
+        int* ve = cols + rowp[v] + g.alen[v];
+        for (int k = 0; k < len; k++) {
+          int* it = std::lower_bound(vb, ve, Lp[k]);
+          if (it != ve && *it == Lp[k]) {
+            vsum[v] -= slen[Lp[k]];
+            rhash[v] -= mix64((uint64_t)Lp[k]);
+            *it = -1;
+            removed_v++;
+            vb = it + 1;
+          } else {
+            vb = it;
+          }
+        }
+      } else {
         int k = 0;
         for (int c = rowp[v] + g.elen[v]; k < len && c < rowp[v] + g.alen[v]; c++) {
           while (k < len && Lp[k] < cols[c]) k++;
@@ -272,6 +321,7 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
         cols[k] = piv;
         g.alen[v] += 1;
         g.elen[v] += 1;
+        if (tracked[v]) rhash[v] += mix64((uint64_t)piv);
       }
     }
 
@@ -315,7 +365,10 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
       const int v = Lp[j];
       if (v == piv) continue;
       int est = deg_lp;
-      for (int k = rowp[v] + g.elen[v]; k < rowp[v] + g.alen[v]; k++) est += slen[cols[k]];
+      if (tracked[v])
+        est += (int)vsum[v];
+      else
+        for (int k = rowp[v] + g.elen[v]; k < rowp[v] + g.alen[v]; k++) est += slen[cols[k]];
       const int vs = rowp[v] + g.elen[v];
       const int vl = g.alen[v] - g.elen[v];
       if (vl > 0 && std::binary_search(cols + vs, cols + vs + vl, v)) est -= slen[v];
@@ -342,6 +395,27 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
     // (Lp[j], Lp[k]), k > j, are tested in order and a match is merged at
     // once (later tests see the merged graph)
     auto merge = [&](int a, int b) {
+      const int sb = slen[b];
+      const int nb = -(a + 1);  // slen[b] after the merge
+      // the long rows that hold a or b see their slen change
+      for (const int t : tracked_list) {
+        if (!tracked[t]) continue;
+        if (in_vars(t, a)) vsum[t] += sb;
+        if (in_vars(t, b)) vsum[t] += (long long)nb - sb;
+      }
+      // the entry drop_variable(b) removes from each neighbour's variable
+      // part: b where it is found before the last entry, else the last entry
+      for (int q = rowp[b] + g.elen[b]; q < rowp[b] + g.alen[b]; q++) {
+        const int w = cols[q];
+        if (w < 0 || w >= n || !tracked[w]) continue;
+        int j = rowp[w] + g.elen[w];
+        const int last = rowp[w] + g.alen[w] - 1;
+        while (j < last && cols[j] != b) j++;
+        const int x = cols[j];
+        vsum[w] -= (x == b) ? nb : (x == a ? slen[a] + sb : slen[x]);
+        rhash[w] -= mix64((uint64_t)x);
+      }
+      tracked[b] = 0;
       slen[a] += slen[b];
       deg.set(a, deg.degree[a] - slen[b]);
       slen[b] = -(a + 1);
@@ -369,36 +443,64 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
       // lookup. A merge changes the rows of the dropped variable's
       // neighbours, whose keys are then recomputed.
       merge_keys.assign(2 * len, 0);
-      by_key[0].clear();
-      by_key[1].clear();
       for (int p = 0; p < len; p++) lp_pos[Lp[p]] = p;
-      auto set_keys = [&](int p) {
+      auto compute_keys = [&](int p) {
         const int v = Lp[p];
         uint64_t r = 0;
-        for (int q = rowp[v]; q < rowp[v] + g.alen[v]; q++) r += mix64((uint64_t)cols[q]);
+        if (tracked[v])
+          r = rhash[v];
+        else
+          for (int q = rowp[v]; q < rowp[v] + g.alen[v]; q++) r += mix64((uint64_t)cols[q]);
         const uint64_t shape = ((uint64_t)(uint32_t)g.alen[v] << 32) | (uint32_t)g.elen[v];
         merge_keys[2 * p] = mix64(r ^ mix64(shape));
         merge_keys[2 * p + 1] = mix64((r + mix64((uint64_t)v)) ^ mix64(shape));
-        by_key[0].insert({merge_keys[2 * p], p});
-        by_key[1].insert({merge_keys[2 * p + 1], p});
       };
-      auto erase_keys = [&](int p) {
-        by_key[0].erase({merge_keys[2 * p], p});
-        by_key[1].erase({merge_keys[2 * p + 1], p});
+      auto active = [&](int p) { return Lp[p] != piv && slen[Lp[p]] >= 0; };
+      // (key, position) sorted, plus the positions re-keyed since the sort;
+      // an entry whose key is no longer its position's current key is stale
+      for (int t = 0; t < 2; t++) {
+        by_key[t].clear();
+        extra[t].clear();
+      }
+      auto rebuild = [&]() {
+        for (int t = 0; t < 2; t++) {
+          by_key[t].clear();
+          extra[t].clear();
+          for (int p = 0; p < len; p++)
+            if (active(p)) by_key[t].push_back({merge_keys[2 * p + t], p});
+          std::sort(by_key[t].begin(), by_key[t].end());
+        }
       };
       for (int p = 0; p < len; p++)
-        if (Lp[p] != piv && slen[Lp[p]] >= 0) set_keys(p);
+        if (active(p)) compute_keys(p);
+      rebuild();
+      auto next_candidate = [&](int j, int k) {
+        int c = INT_MAX;
+        for (int t = 0; t < 2; t++) {
+          const uint64_t key = merge_keys[2 * j + t];
+          auto it = std::lower_bound(by_key[t].begin(), by_key[t].end(),
+                                     std::make_pair(key, k + 1));
+          for (; it != by_key[t].end() && it->first == key; ++it) {
+            const int p = it->second;
+            if (p >= c) break;
+            if (active(p) && merge_keys[2 * p + t] == key) {
+              c = p;
+              break;
+            }
+          }
+          for (const auto& e : extra[t])
+            if (e.first == key && e.second > k && e.second < c && active(e.second) &&
+                merge_keys[2 * e.second + t] == key)
+              c = e.second;
+        }
+        return c;
+      };
       for (int j = 0; j < len; j++) {
         const int a = Lp[j];
         if (a == piv || slen[a] < 0) continue;
         int k = j;
         for (;;) {
-          int c = INT_MAX;
-          for (int t = 0; t < 2; t++) {
-            const uint64_t key = merge_keys[2 * j + t];
-            auto it = by_key[t].lower_bound({key, k + 1});
-            if (it != by_key[t].end() && it->first == key) c = std::min(c, it->second);
-          }
+          const int c = next_candidate(j, k);
           if (c == INT_MAX) break;
           k = c;
           const int b = Lp[k];
@@ -410,12 +512,13 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
             if (w >= 0 && w < n && lp_pos[w] >= 0 && w != piv && slen[w] >= 0 && w != b)
               touched.push_back(lp_pos[w]);
           }
-          erase_keys(k);
           merge(a, b);
           for (const int p : touched) {
-            erase_keys(p);
-            set_keys(p);
+            compute_keys(p);
+            extra[0].push_back({merge_keys[2 * p], p});
+            extra[1].push_back({merge_keys[2 * p + 1], p});
           }
+          if (extra[0].size() > kMergeExtraMax) rebuild();
         }
       }
       for (int p = 0; p < len; p++) lp_pos[Lp[p]] = -1;

@@ -219,3 +219,25 @@ def test_hex_workload_has_the_designed_inertia():
         berr = np.abs(s.matvec(x) - s.rhs).max() / (
             s.inf_norm() * np.abs(x).max() + np.abs(s.rhs).max())
         assert berr < 1e-14
+
+
+def test_symbolic_matches_reference_cliques_and_dense_rows():
+    """Patterns that reach the ordering's long-list paths: many small
+    cliques (repeated ones make indistinguishable variables) and a few dense
+    rows."""
+    rng = np.random.default_rng(123)
+    for _ in range(30):
+        n = int(rng.integers(200, 1500))
+        rows, cols = [], []
+        for _ in range(int(rng.integers(n // 8, n // 2))):
+            m = int(rng.integers(2, 12))
+            vs = rng.choice(n, size=m, replace=False)
+            rows.extend(np.repeat(vs, m))
+            cols.extend(np.tile(vs, m))
+        for _ in range(int(rng.integers(0, 4))):
+            d = int(rng.integers(n))
+            others = rng.choice(n, size=int(rng.integers(n // 3, n)), replace=False)
+            rows.extend([d] * len(others) + list(others))
+            cols.extend(list(others) + [d] * len(others))
+        rowp, colsp, _ = csr_from_coo(n, np.array(rows), np.array(cols), np.ones(len(rows)))
+        _compare_symbolic(rowp, colsp, OrderingType.AMD)
