@@ -207,6 +207,19 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
   std::vector<long long> vsum(n, 0);
   std::vector<uint64_t> rhash(n, 0);
   std::vector<int> tracked_list;
+  // esum[e] = sum of slen over the row of live element e, kept with the row
+  std::vector<long long> esum(n, 0);
+  // slen summed over element e's row (the running sum of a live element)
+  auto element_size = [&](int e) {
+    if (state[e] == 0) return (int)esum[e];
+    int t = 0;
+    for (int p = rowp[e]; p < rowp[e] + g.alen[e]; p++) t += slen[cols[p]];
+    return t;
+  };
+  auto elem_has = [&](int e, int x) {
+    const int* b = cols + rowp[e];
+    return std::binary_search(b, b + g.alen[e], x);
+  };
   for (int v = 0; v < n; v++)
     if (g.alen[v] > kTrackRow) tracked_list.push_back(v);
   // the longest few only: every merge checks each tracked row
@@ -345,6 +358,9 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
       }
       cols[j] = Lp[k];
     }
+    esum[piv] = 0;
+    for (int k = 0; k < len; k++)
+      if (Lp[k] != piv) esum[piv] += slen[Lp[k]];
 
     // approximate external degrees |A_v \ v| + |Lp \ v| + sum_e |L_e \ Lp|
     for (int j = 0; j < len; j++) {
@@ -352,8 +368,7 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
       for (int k = rowp[v]; k < rowp[v] + g.elen[v]; k++) {
         const int e = cols[k];
         if (elem_deg[e] < 0) {
-          elem_deg[e] = 0;
-          for (int p = rowp[e]; p < rowp[e] + g.alen[e]; p++) elem_deg[e] += slen[cols[p]];
+          elem_deg[e] = element_size(e);
         }
         elem_deg[e] -= slen[v];
       }
@@ -361,6 +376,7 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
     int deg_lp = 0;
     for (int j = 0; j < len; j++)
       if (Lp[j] != piv) deg_lp += slen[Lp[j]];
+
     for (int j = 0; j < len; j++) {
       const int v = Lp[j];
       if (v == piv) continue;
@@ -377,8 +393,7 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
         const int e = cols[k];
         if (e == piv) continue;
         if (elem_deg[e] < 0) {
-          elem_deg[e] = 0;
-          for (int p = rowp[e]; p < rowp[e] + g.alen[e]; p++) elem_deg[e] += slen[cols[p]];
+          elem_deg[e] = element_size(e);
         }
         est += elem_deg[e];
       }
@@ -402,6 +417,24 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
         if (!tracked[t]) continue;
         if (in_vars(t, a)) vsum[t] += sb;
         if (in_vars(t, b)) vsum[t] += (long long)nb - sb;
+      }
+      // live elements holding a or b see their slen change; every element
+      // that holds a variable is in that variable's element list
+      for (int q = rowp[a]; q < rowp[a] + g.elen[a]; q++) {
+        const int e = cols[q];
+        if (state[e] == 0 && elem_has(e, a)) esum[e] += sb;
+      }
+      for (int q = rowp[b]; q < rowp[b] + g.elen[b]; q++) {
+        const int e = cols[q];
+        if (state[e] != 0) continue;
+        if (elem_has(e, b)) esum[e] += (long long)nb - sb;
+        // the entry drop_variable(b) removes from e's row
+        int j = rowp[e];
+        const int last = rowp[e] + g.alen[e] - 1;
+        if (last < j) continue;
+        while (j < last && cols[j] != b) j++;
+        const int x = cols[j];
+        esum[e] -= (x == b) ? nb : (x == a ? slen[a] + sb : slen[x]);
       }
       // the entry drop_variable(b) removes from each neighbour's variable
       // part: b where it is found before the last entry, else the last entry
