@@ -241,7 +241,7 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
   // supervariable detection on long lists (see the merge step)
   std::vector<int> lp_pos(n, -1), touched;
   std::vector<uint64_t> merge_keys;
-  std::vector<std::pair<uint64_t, int>> by_key[2], extra[2];
+  std::vector<int> head[2], chain[2], extra[2];
   int nsv = 0;
   for (int i = 0; i < n; nsv++) {
     const int piv = deg.pick();
@@ -489,19 +489,23 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
         merge_keys[2 * p + 1] = mix64((r + mix64((uint64_t)v)) ^ mix64(shape));
       };
       auto active = [&](int p) { return Lp[p] != piv && slen[Lp[p]] >= 0; };
-      // (key, position) sorted, plus the positions re-keyed since the sort;
-      // an entry whose key is no longer its position's current key is stale
-      for (int t = 0; t < 2; t++) {
-        by_key[t].clear();
-        extra[t].clear();
-      }
+      // Per key kind: a hash table of chains of positions in increasing
+      // order (filled from the back), plus the positions re-keyed since it
+      // was filled. An entry whose key is no longer its position's current
+      // key is stale and skipped.
+      int tsize = 1;
+      while (tsize < 2 * len) tsize <<= 1;
       auto rebuild = [&]() {
         for (int t = 0; t < 2; t++) {
-          by_key[t].clear();
+          head[t].assign(tsize, -1);
+          chain[t].assign(len, -1);
           extra[t].clear();
-          for (int p = 0; p < len; p++)
-            if (active(p)) by_key[t].push_back({merge_keys[2 * p + t], p});
-          std::sort(by_key[t].begin(), by_key[t].end());
+          for (int p = len - 1; p >= 0; p--) {
+            if (!active(p)) continue;
+            const int slot = (int)(merge_keys[2 * p + t] & (uint64_t)(tsize - 1));
+            chain[t][p] = head[t][slot];
+            head[t][slot] = p;
+          }
         }
       };
       for (int p = 0; p < len; p++)
@@ -511,20 +515,15 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
         int c = INT_MAX;
         for (int t = 0; t < 2; t++) {
           const uint64_t key = merge_keys[2 * j + t];
-          auto it = std::lower_bound(by_key[t].begin(), by_key[t].end(),
-                                     std::make_pair(key, k + 1));
-          for (; it != by_key[t].end() && it->first == key; ++it) {
-            const int p = it->second;
-            if (p >= c) break;
-            if (active(p) && merge_keys[2 * p + t] == key) {
+          for (int p = head[t][(int)(key & (uint64_t)(tsize - 1))]; p >= 0 && p < c;
+               p = chain[t][p]) {
+            if (p > k && merge_keys[2 * p + t] == key && active(p)) {
               c = p;
               break;
             }
           }
-          for (const auto& e : extra[t])
-            if (e.first == key && e.second > k && e.second < c && active(e.second) &&
-                merge_keys[2 * e.second + t] == key)
-              c = e.second;
+          for (const int p : extra[t])
+            if (p > k && p < c && merge_keys[2 * p + t] == key && active(p)) c = p;
         }
         return c;
       };
@@ -548,8 +547,8 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
           merge(a, b);
           for (const int p : touched) {
             compute_keys(p);
-            extra[0].push_back({merge_keys[2 * p], p});
-            extra[1].push_back({merge_keys[2 * p + 1], p});
+            extra[0].push_back(p);
+            extra[1].push_back(p);
           }
           if (extra[0].size() > kMergeExtraMax) rebuild();
         }
