@@ -269,7 +269,22 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
       const int v = Lp[j];
       if (v == piv) continue;
       int removed_e = 0;
-      {
+      if (tracked[v]) {
+        // the same entries by binary search over v's (sorted) element part
+        int* eb = cols + rowp[v];
+        int* ee = cols + rowp[v] + g.elen[v];
+        for (int k = rowp[piv]; k < rowp[piv] + g.elen[piv]; k++) {
+          int* it = std::lower_bound(eb, ee, cols[k]);
+          if (it != ee && *it == cols[k]) {
+            rhash[v] -= mix64((uint64_t)*it);
+            *it = -1;
+            removed_e++;
+            eb = it + 1;
+          } else {
+            eb = it;
+          }
+        }
+      } else {
         int k = rowp[piv];
         const int kend = rowp[piv] + g.elen[piv];
         for (int c = rowp[v]; k < kend && c < rowp[v] + g.elen[v]; c++) {
