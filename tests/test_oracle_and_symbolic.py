@@ -241,3 +241,20 @@ def test_symbolic_matches_reference_cliques_and_dense_rows():
             cols.extend(list(others) + [d] * len(others))
         rowp, colsp, _ = csr_from_coo(n, np.array(rows), np.array(cols), np.ones(len(rows)))
         _compare_symbolic(rowp, colsp, OrderingType.AMD)
+
+
+def test_generated_kkt_systems_are_symmetric_with_diagonals():
+    """Every workload's CSR holds the full symmetric pattern with exactly
+    symmetric values, a diagonal entry in every row and sorted columns."""
+    from amigo_b200.workloads import hex_elasticity_kkt
+
+    for s in (optimal_control_kkt(N=50), plane_stress_kkt(6), hex_elasticity_kkt(3),
+              *batched_optimal_control(num_systems=2, seed=1)):
+        n = s.n
+        r = np.repeat(np.arange(n), np.diff(s.rowp))
+        a = {(int(i), int(j)): v for i, j, v in zip(r, s.cols, s.vals)}
+        assert all(a.get((j, i)) == v for (i, j), v in a.items()), s.name
+        assert all((i, i) in a for i in range(n)), s.name
+        for i in range(n):
+            c = s.cols[s.rowp[i]:s.rowp[i + 1]]
+            assert np.all(np.diff(c) > 0), s.name
