@@ -216,6 +216,17 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
     for (int p = rowp[e]; p < rowp[e] + g.alen[e]; p++) t += slen[cols[p]];
     return t;
   };
+  // For a long row T: esumT[T] = sum over T's elements of their slen sums
+  // (0 for a dead element), kept with T's element part and with esum.
+  std::vector<long long> esumT(n, 0), corr(n, 0);
+  std::vector<int> tl;  // long rows in the current Lp
+  // held[e] bit b: the long row tracked_list[b] holds element e (set and
+  // cleared with the row's element part: insertion of a new element, prune
+  // of absorbed ones)
+  std::vector<uint64_t> held(n, 0);
+  std::vector<int> tbit(n, -1);
+  auto elem_in = [&](int t, int e) { return (held[e] >> tbit[t]) & 1u; };
+  auto elem_value = [&](int e) { return state[e] == 0 ? esum[e] : 0LL; };
   auto elem_has = [&](int e, int x) {
     const int* b = cols + rowp[e];
     return std::binary_search(b, b + g.alen[e], x);
@@ -226,6 +237,7 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
   std::stable_sort(tracked_list.begin(), tracked_list.end(),
                    [&](int x, int y) { return g.alen[x] > g.alen[y]; });
   if (tracked_list.size() > (size_t)kTrackMaxRows) tracked_list.resize(kTrackMaxRows);
+  for (size_t b = 0; b < tracked_list.size(); b++) tbit[tracked_list[b]] = (int)b;
   for (const int v : tracked_list) {
     tracked[v] = 1;
     for (int q = rowp[v]; q < rowp[v] + g.alen[v]; q++) {
@@ -277,6 +289,8 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
           int* it = std::lower_bound(eb, ee, cols[k]);
           if (it != ee && *it == cols[k]) {
             rhash[v] -= mix64((uint64_t)*it);
+            esumT[v] -= elem_value(*it);
+            held[*it] &= ~(1ull << tbit[v]);
             *it = -1;
             removed_e++;
             eb = it + 1;
@@ -349,13 +363,20 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
         cols[k] = piv;
         g.alen[v] += 1;
         g.elen[v] += 1;
-        if (tracked[v]) rhash[v] += mix64((uint64_t)piv);
+        if (tracked[v]) {
+          rhash[v] += mix64((uint64_t)piv);
+          held[piv] |= 1ull << tbit[v];
+        }
       }
     }
 
     // the elements adjacent to piv are absorbed into it
     for (int j = rowp[piv]; j < rowp[piv] + g.elen[piv]; j++) {
       const int e = cols[j];
+      for (uint64_t m = held[e]; m; m &= m - 1) {
+        const int t = tracked_list[__builtin_ctzll(m)];
+        if (tracked[t]) esumT[t] -= elem_value(e);
+      }
       g.alen[e] = 0;
       g.elen[e] = 0;
       state[e] = -1;
@@ -376,16 +397,53 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
     esum[piv] = 0;
     for (int k = 0; k < len; k++)
       if (Lp[k] != piv) esum[piv] += slen[Lp[k]];
+    for (int k = 0; k < len; k++)
+      if (Lp[k] != piv && tracked[Lp[k]]) esumT[Lp[k]] += esum[piv];
 
-    // approximate external degrees |A_v \ v| + |Lp \ v| + sum_e |L_e \ Lp|
+    // approximate external degrees |A_v \ v| + |Lp \ v| + sum_e |L_e \ Lp|.
+    // elem_deg[e] = |L_e| minus slen of every member of Lp holding e. A long
+    // row T in Lp does not walk its elements: each element's first visitor
+    // subtracts slen[T] when T holds it, and T's own sum comes from esumT
+    // minus corr[T] = sum over T's elements of the slen of the Lp members
+    // that hold them.
+    tl.clear();
+    for (int j = 0; j < len; j++)
+      if (Lp[j] != piv && tracked[Lp[j]]) tl.push_back(Lp[j]);
+    for (const int t : tl) {
+      corr[t] = (long long)slen[t] * g.elen[t];
+      for (const int u : tl) {
+        if (u == t) continue;
+        // |elements(t) and elements(u)| by a merge of the sorted lists
+        long long both = 0;
+        int x = rowp[t], y = rowp[u];
+        const int xe = rowp[t] + g.elen[t], ye = rowp[u] + g.elen[u];
+        while (x < xe && y < ye) {
+          if (cols[x] < cols[y])
+            x++;
+          else if (cols[y] < cols[x])
+            y++;
+          else {
+            both++;
+            x++;
+            y++;
+          }
+        }
+        corr[t] += (long long)slen[u] * both;
+      }
+    }
     for (int j = 0; j < len; j++) {
       const int v = Lp[j];
+      if (v != piv && tracked[v]) continue;
       for (int k = rowp[v]; k < rowp[v] + g.elen[v]; k++) {
         const int e = cols[k];
         if (elem_deg[e] < 0) {
           elem_deg[e] = element_size(e);
+          for (const int t : tl)
+            if (elem_in(t, e)) elem_deg[e] -= slen[t];
         }
         elem_deg[e] -= slen[v];
+        for (const int t : tl)
+          if (elem_in(t, e)) corr[t] += slen[v];
       }
     }
     int deg_lp = 0;
@@ -404,13 +462,18 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
       const int vl = g.alen[v] - g.elen[v];
       if (vl > 0 && std::binary_search(cols + vs, cols + vs + vl, v)) est -= slen[v];
       if (std::binary_search(Lp.data(), Lp.data() + len, v)) est -= slen[v];
-      for (int k = rowp[v]; k < rowp[v] + g.elen[v]; k++) {
-        const int e = cols[k];
-        if (e == piv) continue;
-        if (elem_deg[e] < 0) {
-          elem_deg[e] = element_size(e);
+      if (tracked[v]) {
+        // piv's own term is |L_piv| - deg_lp, zero, and is excluded
+        est += (int)(esumT[v] - corr[v] - (esum[piv] - deg_lp));
+      } else {
+        for (int k = rowp[v]; k < rowp[v] + g.elen[v]; k++) {
+          const int e = cols[k];
+          if (e == piv) continue;
+          if (elem_deg[e] < 0) {
+            elem_deg[e] = element_size(e);
+          }
+          est += elem_deg[e];
         }
-        est += elem_deg[e];
       }
       est = std::min(est, n - i);
       const int d = std::min(est, deg.degree[v] + deg_lp);
@@ -418,6 +481,7 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
     }
     for (int j = 0; j < len; j++) {
       const int v = Lp[j];
+      if (v != piv && tracked[v]) continue;  // its elements were set by others, if at all
       for (int k = rowp[v]; k < rowp[v] + g.elen[v]; k++) elem_deg[cols[k]] = -1;
     }
 
@@ -437,19 +501,33 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
       // that holds a variable is in that variable's element list
       for (int q = rowp[a]; q < rowp[a] + g.elen[a]; q++) {
         const int e = cols[q];
-        if (state[e] == 0 && elem_has(e, a)) esum[e] += sb;
+        if (state[e] == 0 && elem_has(e, a)) {
+          esum[e] += sb;
+          for (uint64_t m = held[e]; m; m &= m - 1) {
+            const int t = tracked_list[__builtin_ctzll(m)];
+            if (tracked[t]) esumT[t] += sb;
+          }
+        }
       }
       for (int q = rowp[b]; q < rowp[b] + g.elen[b]; q++) {
         const int e = cols[q];
         if (state[e] != 0) continue;
-        if (elem_has(e, b)) esum[e] += (long long)nb - sb;
+        long long delta = 0;
+        if (elem_has(e, b)) delta += (long long)nb - sb;
         // the entry drop_variable(b) removes from e's row
         int j = rowp[e];
         const int last = rowp[e] + g.alen[e] - 1;
-        if (last < j) continue;
-        while (j < last && cols[j] != b) j++;
-        const int x = cols[j];
-        esum[e] -= (x == b) ? nb : (x == a ? slen[a] + sb : slen[x]);
+        if (last >= j) {
+          while (j < last && cols[j] != b) j++;
+          const int x = cols[j];
+          delta -= (x == b) ? nb : (x == a ? slen[a] + sb : slen[x]);
+        }
+        esum[e] += delta;
+        if (delta != 0)
+          for (uint64_t m = held[e]; m; m &= m - 1) {
+            const int t = tracked_list[__builtin_ctzll(m)];
+            if (tracked[t]) esumT[t] += delta;
+          }
       }
       // the entry drop_variable(b) removes from each neighbour's variable
       // part: b where it is found before the last entry, else the last entry
