@@ -572,7 +572,8 @@ int b200ldl_create(b200ldl_t* out, int n, int nnz, const int* rowp, const int* c
   *out = nullptr;
   if (n < 0 || nnz < 0 || (n > 0 && (!rowp || !cols))) return -1;
   if (solver_type != B200LDL_LDL && solver_type != B200LDL_CHOLESKY) return -1;
-  if (order < 0 || order > 3 || order == B200LDL_ORDER_MULTI_COLOR) return -1;
+  if (order < 0 || order > B200LDL_ORDER_GRAPH_ND || order == B200LDL_ORDER_MULTI_COLOR)
+    return -1;
   if (n > 0 && (rowp[0] != 0 || rowp[n] != nnz)) return -1;
   for (int i = 0; i < n; i++)
     if (rowp[i + 1] < rowp[i]) return -1;
@@ -608,7 +609,8 @@ int b200ldl_create_batch(b200ldl_t* out, int nsys, const int* sys_n, const int* 
   *out = nullptr;
   if (nsys < 1 || !sys_n || !sys_nnz || !rowp_cat || !cols_cat) return -1;
   if (solver_type != B200LDL_LDL && solver_type != B200LDL_CHOLESKY) return -1;
-  if (order < 0 || order > 3 || order == B200LDL_ORDER_MULTI_COLOR) return -1;
+  if (order < 0 || order > B200LDL_ORDER_GRAPH_ND || order == B200LDL_ORDER_MULTI_COLOR)
+    return -1;
   // validate every system and build the block-diagonal pattern
   long long ntot = 0, nztot = 0;
   {

@@ -8,6 +8,7 @@
 #include "symbolic.h"
 
 #include <algorithm>
+#include <cmath>
 #include <climits>
 #include <cstdint>
 #include <utility>
@@ -671,6 +672,214 @@ int amd_order(int n, int* rowp, int* cols, int* perm) {
   return 0;
 }
 
+namespace {
+
+// parts of at most this many vertices are ordered by AMD on their subgraph
+constexpr int kNdLeaf = 256;
+
+// AMD on the subgraph induced by `verts` (adjacency adj/adj_ptr, global
+// ids); appends the vertices in elimination order to `out`.
+void amd_subgraph(const std::vector<int>& verts, const std::vector<int>& adj_ptr,
+                  const std::vector<int>& adj, std::vector<int>& local,
+                  std::vector<int>& out) {
+  const int m = (int)verts.size();
+  for (int i = 0; i < m; i++) local[verts[i]] = i;
+  std::vector<int> rp(m + 1, 0), cc;
+  for (int i = 0; i < m; i++) {
+    const int v = verts[i];
+    const size_t start = cc.size();
+    cc.push_back(i);
+    for (int q = adj_ptr[v]; q < adj_ptr[v + 1]; q++) {
+      const int w = local[adj[q]];
+      if (w >= 0) cc.push_back(w);
+    }
+    std::sort(cc.begin() + start, cc.end());
+    cc.erase(std::unique(cc.begin() + start, cc.end()), cc.end());
+    rp[i + 1] = (int)cc.size();
+  }
+  std::vector<int> p(m);
+  if (amd_order(m, rp.data(), cc.data(), p.data()) != 0) std::iota(p.begin(), p.end(), 0);
+  for (int i = 0; i < m; i++) out.push_back(verts[p[i]]);
+  for (int i = 0; i < m; i++) local[verts[i]] = -1;
+}
+
+}  // namespace
+
+// Nested dissection without METIS (our own ordering, not the reference's:
+// without METIS the reference's nested dissection is the identity). Rows
+// far denser than the rest (e.g. a constraint on every design variable) are
+// set aside and ordered last. The rest is split recursively: a breadth-first
+// level structure from a pseudo-peripheral vertex, the level that halves
+// the part as the separator, thinned to the vertices with a neighbour in
+// the next level. Each separator follows its two parts; parts of at most
+// kNdLeaf vertices are ordered by AMD on their subgraph.
+void nd_order(int n, const int* rowp, const int* cols, int* perm) {
+  // adjacency without the diagonal
+  std::vector<int> adj_ptr(n + 1, 0), adj;
+  adj.reserve(rowp[n]);
+  for (int i = 0; i < n; i++) {
+    for (int q = rowp[i]; q < rowp[i + 1]; q++)
+      if (cols[q] != i && cols[q] >= 0 && cols[q] < n) adj.push_back(cols[q]);
+    adj_ptr[i + 1] = (int)adj.size();
+  }
+  long long total = adj_ptr[n];
+  const double avg = n > 0 ? (double)total / n : 0.0;
+  const int dense_min = std::max(64, (int)std::max(10.0 * avg, 10.0 * std::sqrt((double)n)));
+  std::vector<int> part(n, 0), level(n, -1), local(n, -1), dense;
+  for (int v = 0; v < n; v++) {
+    if (adj_ptr[v + 1] - adj_ptr[v] > dense_min) {
+      part[v] = -1;  // set aside
+      dense.push_back(v);
+    }
+  }
+  std::vector<int> out;
+  out.reserve(n);
+  // explicit stack of tasks: a part to split (verts, id) or a separator to emit
+  struct Task {
+    std::vector<int> verts;
+    int id;
+    bool emit;
+  };
+  std::vector<Task> stack;
+  {
+    Task t{{}, 0, false};
+    for (int v = 0; v < n; v++)
+      if (part[v] == 0) t.verts.push_back(v);
+    stack.push_back(std::move(t));
+  }
+  int next_id = 1;
+  std::vector<int> queue;
+  auto bfs = [&](int root, int id, std::vector<int>& order) {
+    order.clear();
+    order.push_back(root);
+    level[root] = 0;
+    for (size_t h = 0; h < order.size(); h++) {
+      const int v = order[h];
+      for (int q = adj_ptr[v]; q < adj_ptr[v + 1]; q++) {
+        const int w = adj[q];
+        if (part[w] == id && level[w] < 0) {
+          level[w] = level[v] + 1;
+          order.push_back(w);
+        }
+      }
+    }
+  };
+  auto clear_levels = [&](const std::vector<int>& vs) {
+    for (const int v : vs) level[v] = -1;
+  };
+  while (!stack.empty()) {
+    Task t = std::move(stack.back());
+    stack.pop_back();
+    if (t.emit) {
+      for (const int v : t.verts) out.push_back(v);
+      continue;
+    }
+    const int m = (int)t.verts.size();
+    if (m == 0) continue;
+    if (m <= kNdLeaf) {
+      amd_subgraph(t.verts, adj_ptr, adj, local, out);
+      for (const int v : t.verts) part[v] = -2;  // done
+      continue;
+    }
+    // the component of t.verts[0]; other components become their own part
+    bfs(t.verts[0], t.id, queue);
+    if ((int)queue.size() < m) {
+      Task rest{{}, next_id++, false};
+      for (const int v : t.verts)
+        if (level[v] < 0) {
+          part[v] = rest.id;
+          rest.verts.push_back(v);
+        }
+      Task comp{queue, next_id++, false};
+      clear_levels(queue);
+      for (const int v : comp.verts) part[v] = comp.id;
+      stack.push_back(std::move(rest));
+      stack.push_back(std::move(comp));
+      continue;
+    }
+    // pseudo-peripheral root: restart from a far vertex of least degree
+    int height = level[queue.back()];
+    for (int it = 0; it < 4; it++) {
+      int best = queue.back();
+      for (size_t h = queue.size(); h-- > 0;) {
+        const int v = queue[h];
+        if (level[v] < height) break;
+        if (adj_ptr[v + 1] - adj_ptr[v] < adj_ptr[best + 1] - adj_ptr[best]) best = v;
+      }
+      clear_levels(queue);
+      bfs(best, t.id, queue);
+      const int h2 = level[queue.back()];
+      if (h2 <= height) break;
+      height = h2;
+    }
+    // among the levels that leave 35-65% of the part on their lower side,
+    // the one with the fewest vertices touching the next level
+    int mid = 0;
+    {
+      std::vector<int> below(height + 2, 0), thin(height + 2, 0);
+      for (const int v : queue) {
+        const int l = level[v];
+        below[l + 1]++;
+        bool touches_next = false;
+        for (int q = adj_ptr[v]; q < adj_ptr[v + 1] && !touches_next; q++) {
+          const int w = adj[q];
+          touches_next = (part[w] == t.id && level[w] == l + 1);
+        }
+        thin[l] += touches_next;
+      }
+      for (int l = 1; l <= height + 1; l++) below[l] += below[l - 1];
+      int best = -1;
+      for (int l = 1; l < height; l++) {
+        const long long lo = below[l];  // vertices in levels < l
+        if (20 * lo < 7 * (long long)m || 20 * lo > 13 * (long long)m) continue;
+        if (best < 0 || thin[l] < thin[best]) best = l;
+      }
+      if (best < 0) {
+        int cum = 0;
+        for (size_t h = 0; h < queue.size(); h++) {
+          cum++;
+          if (2 * cum >= m) {
+            best = level[queue[h]];
+            break;
+          }
+        }
+      }
+      mid = best;
+    }
+    if (mid == 0 || mid >= height) {  // no useful split: order the part by AMD
+      clear_levels(queue);
+      amd_subgraph(t.verts, adj_ptr, adj, local, out);
+      for (const int v : t.verts) part[v] = -2;
+      continue;
+    }
+    Task a{{}, next_id++, false}, b{{}, next_id++, false}, sep{{}, -1, true};
+    for (const int v : queue) {
+      const int l = level[v];
+      if (l < mid) {
+        a.verts.push_back(v);
+      } else if (l > mid) {
+        b.verts.push_back(v);
+      } else {
+        bool touches_next = false;
+        for (int q = adj_ptr[v]; q < adj_ptr[v + 1] && !touches_next; q++) {
+          const int w = adj[q];
+          touches_next = (part[w] == t.id && level[w] == mid + 1);
+        }
+        (touches_next ? sep.verts : a.verts).push_back(v);
+      }
+    }
+    clear_levels(queue);
+    for (const int v : a.verts) part[v] = a.id;
+    for (const int v : b.verts) part[v] = b.id;
+    for (const int v : sep.verts) part[v] = -2;
+    stack.push_back(std::move(sep));  // emitted after both parts
+    stack.push_back(std::move(b));
+    stack.push_back(std::move(a));
+  }
+  for (const int v : dense) out.push_back(v);
+  for (int i = 0; i < n; i++) perm[i] = out[i];
+}
+
 // copy_for_reorder (ordering_utils.h:313-360) + reorder (38-56): AMD sees the
 // pattern with the diagonal added, rows sorted and de-duplicated in place;
 // nested dissection without METIS is the identity (189-194).
@@ -710,6 +919,8 @@ void compute_ordering(Ordering order, int n, const int* rowp, const int* cols,
       std::fprintf(stderr, "b200ldl: AMD input format error at row %d\n", flag - 1);
       std::iota(perm.begin(), perm.end(), 0);
     }
+  } else if (order == Ordering::GraphNd) {
+    nd_order(n, rowp, cols, perm.data());
   } else if (order == Ordering::MultiColor) {
     throw std::invalid_argument("multicolor ordering is not supported");
   } else {

@@ -12,7 +12,16 @@
 
 namespace b200ldl {
 
-enum class Ordering : int { NestedDissection = 0, Amd = 1, MultiColor = 2, Natural = 3 };
+// NestedDissection..Natural as the reference numbers them (nested
+// dissection without METIS is the identity there); GraphNd is our own
+// nested dissection (nd_order).
+enum class Ordering : int {
+  NestedDissection = 0,
+  Amd = 1,
+  MultiColor = 2,
+  Natural = 3,
+  GraphNd = 4
+};
 
 struct Symbolic {
   int n = 0;
@@ -36,6 +45,10 @@ struct Symbolic {
 // diagonal, any column order).
 void compute_ordering(Ordering order, int n, const int* rowp, const int* cols,
                       std::vector<int>& perm, std::vector<int>& iperm);
+
+// Nested dissection of the full symmetric pattern without METIS; perm[k] =
+// k-th vertex eliminated.
+void nd_order(int n, const int* rowp, const int* cols, int* perm);
 
 // Approximate minimum degree on a prepared quotient-graph CSR (diagonal
 // present, sorted, unique). rowp/cols are modified. perm[k] = k-th pivot.

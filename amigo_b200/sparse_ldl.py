@@ -35,6 +35,9 @@ class OrderingType(enum.IntEnum):
     AMD = 1
     MULTI_COLOR = 2
     NATURAL = 3
+    # our nested dissection without METIS (the reference's needs METIS and
+    # is the identity without it); not one of the reference's values
+    GRAPH_ND = 4
     # the reference's DEFAULT without METIS (amigo/amigo.cpp:329-333)
     DEFAULT = 1
 

@@ -38,6 +38,10 @@ typedef struct b200ldl_handle* b200ldl_t;
 #define B200LDL_ORDER_AMD 1
 #define B200LDL_ORDER_MULTI_COLOR 2
 #define B200LDL_ORDER_NATURAL 3
+/* Our own nested dissection without METIS (no counterpart in the reference,
+ * whose nested dissection needs METIS): dense rows last, recursive
+ * separators from breadth-first level structures, AMD on small parts. */
+#define B200LDL_ORDER_GRAPH_ND 4
 
 /* Create a solver for a fixed sparsity pattern and run the symbolic phase on
  * the host (ordering, elimination tree, supernodes, contribution rows), then

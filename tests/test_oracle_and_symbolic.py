@@ -258,3 +258,58 @@ def test_generated_kkt_systems_are_symmetric_with_diagonals():
         for i in range(n):
             c = s.cols[s.rowp[i]:s.rowp[i + 1]]
             assert np.all(np.diff(c) > 0), s.name
+
+
+def _permuted_csr(rowp, cols, iperm):
+    n = len(rowp) - 1
+    r = np.repeat(np.arange(n), np.diff(rowp))
+    rp, cp, _ = csr_from_coo(n, iperm[r], iperm[cols], np.ones(len(r)))
+    return rp, cp
+
+
+def test_graph_nd_gives_a_permutation_on_awkward_patterns():
+    rng = np.random.default_rng(5)
+    cases = [(1, [0], [0]), (6, [0, 1, 3, 4], [1, 0, 4, 3])]
+    for _ in range(20):
+        n = int(rng.integers(50, 1500))
+        a = rng.random((n, n)) < rng.random() * 0.02
+        a = a | a.T
+        if rng.random() < 0.5:  # a dense row
+            d = int(rng.integers(n))
+            a[d, :] = a[:, d] = True
+        r, c = np.nonzero(a)
+        cases.append((n, r, c))
+    for n, r, c in cases:
+        rowp, cols, _ = csr_from_coo(n, np.asarray(r), np.asarray(c), np.ones(len(r)))
+        inv = SparseLDL(CSRMat(n, n, rowp, cols), order=OrderingType.GRAPH_ND).symbolic()["invperm"]
+        assert sorted(inv.tolist()) == list(range(n))
+
+
+def test_symbolic_under_graph_nd_is_the_references_on_the_permuted_matrix():
+    """With our nested dissection, the supernodes, children and contribution
+    rows equal the reference's symbolic phase run on the symmetrically
+    permuted matrix in natural order (mapped back through the permutation);
+    and the reference factors that matrix with the designed inertia."""
+    from amigo_b200.workloads import hex_elasticity_kkt
+
+    for s in (plane_stress_kkt(16), hex_elasticity_kkt(6)):
+        a = SparseLDL(CSRMat(s.n, s.n, s.rowp, s.cols), order=OrderingType.GRAPH_ND).symbolic()
+        inv = a["invperm"]
+        perm = np.argsort(inv)
+        rp, cp = _permuted_csr(s.rowp, s.cols, inv)
+        b = ref.RefLDL(rp, cp, order=ref.ORDER_NATURAL).symbolic()
+        assert np.array_equal(a["node_ptr"], b["node_ptr"])
+        assert np.array_equal(a["node_to_var"], perm[b["node_to_var"]])
+        assert np.array_equal(a["children_ptr"], b["children_ptr"])
+        assert np.array_equal(a["children"], b["children"])
+        assert np.array_equal(a["contrib_ptr"], b["contrib_ptr"])
+        assert np.array_equal(a["contrib_rows"], perm[b["contrib_rows"]])
+        # the permuted system itself
+        r_ = np.repeat(np.arange(s.n), np.diff(s.rowp))
+        key = inv[r_].astype(np.int64) * s.n + inv[s.cols]
+        vals = np.empty(len(key))
+        order_ = np.argsort(key)
+        vals[:] = s.vals[order_]  # CSR of P A P^T lists entries in sorted key order
+        r = ref.RefLDL(rp, cp, order=ref.ORDER_NATURAL)
+        r.factor(vals, s.diag[perm])
+        assert tuple(r.inertia()) == s.expected_inertia
