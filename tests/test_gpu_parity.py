@@ -186,3 +186,18 @@ def test_hex_elasticity_with_dense_row(nel):
     from amigo_b200.workloads import hex_elasticity_kkt
 
     _check_system(hex_elasticity_kkt(nel), fwd_tol=1e-4)
+
+
+def test_graph_nd_ordering():
+    # our nested dissection without METIS: inertia is the designed one (it
+    # does not depend on the ordering) and the backward error stays at FP64
+    from amigo_b200.workloads import hex_elasticity_kkt
+
+    for s in (plane_stress_kkt(32), hex_elasticity_kkt(8), plane_stress_kkt(96)):
+        g = _gpu(s.rowp, s.cols, OrderingType.GRAPH_ND)
+        g.mat.vals = s.vals
+        assert g.factor(Vector(s.diag)) == 0
+        assert tuple(g.get_inertia()) == s.expected_inertia, s.name
+        x = np.asfortranarray(s.rhs.copy())
+        g.solve(x)
+        assert backward_error(s, x, s.rhs) <= BERR_TOL, s.name
