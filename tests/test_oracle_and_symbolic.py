@@ -199,7 +199,7 @@ def test_symbolic_matches_reference_hex_with_dense_row(order):
     """The 3D workload with its dense volume-constraint row, at small sizes."""
     from amigo_b200.workloads import hex_elasticity_kkt
 
-    for nel in (2, 4, 6):
+    for nel in (2, 4, 6, 10):
         s = hex_elasticity_kkt(nel)
         _compare_symbolic(s.rowp, s.cols, order)
 
