@@ -37,6 +37,23 @@ L2_BYTES = 126 * 1024 * 1024
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
 
+def host_info() -> dict:
+    """The host the CPU baseline ran on: CPU model, logical cores, and the
+    BLAS the compiled reference links (OpenBLAS from the image's opencv
+    wheel, see oracle/Makefile)."""
+    cpu = "unknown"
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    cpu = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu": cpu, "nproc": os.cpu_count() or 1,
+            "blas": "OpenBLAS 0.3.15 (LP64, opencv-python-headless wheel)"}
+
+
 def load_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -185,7 +202,7 @@ def run_reference(args, world, rank):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"plane-stress KKT {args.nel}x{args.nel} (n={s.n}, nnz={s.nnz}), "
                                "5 RHS, AMD", "nrhs": 5, "parallelism": "host OpenMP"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "host": host_info(),
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "inertia": list(inertia), "backward_error": berr,
@@ -259,7 +276,7 @@ def run_reference_batched(args, world, rank):
                                "one RHS each, AMD, FP64",
                    "parallelism": f"one system per host thread, {cores} threads"},
         "cpu_baseline": {"value": value, "unit": "batch factor+solve/s", "cores": cores,
-                         "kind": "reference",
+                         "kind": "reference", "host": host_info(),
                          "sample": f"systems completed within {per_step:.0f} s per step, "
                                    "scaled to the batch"},
         "e2e": {"value": value, "unit": "batch factor+solve/s", "h2d_bytes_per_step": 0,
@@ -451,7 +468,7 @@ def run_ours(args, world, rank, local):
         if ref.available():
             times, cinertia, _ = cpu_reference_sample(s, 1, 30.0, 1, 0)
             cms = 1e3 * float(np.mean(times))
-            cpu = {"value": 1e3 / cms, "unit": UNIT, "cores": 1, "kind": "reference",
+            cpu = {"value": 1e3 / cms, "unit": UNIT, "cores": 1, "kind": "reference", "host": host_info(),
                    "sample": f"{len(times)} factor+5-RHS solve of the full system, serial "
                              "build, OPENBLAS_NUM_THREADS=1",
                    "inertia": list(cinertia)}
@@ -578,7 +595,7 @@ def run_batched(args, world, rank, local):
                     break
             per_batch = done / n_done * len(all_systems)
             cpu = {"value": 1.0 / per_batch, "unit": "batch factor+solve/s", "cores": 1,
-                   "kind": "reference",
+                   "kind": "reference", "host": host_info(),
                    "sample": f"{n_done} of {len(all_systems)} systems, serial, scaled to the batch"}
     n_total = sum(q.n for q in all_systems)
     line = {

@@ -30,6 +30,7 @@ def _check_reference_line(line):
     assert line["cpu_baseline"]["kind"] == "reference"
     assert line["cpu_baseline"]["value"] == line["value"]
     assert line["cpu_baseline"]["cores"] >= 1
+    assert line["cpu_baseline"]["host"]["nproc"] >= 1
     assert line["backward_error"] < 1e-10
 
 
