@@ -36,6 +36,10 @@ SIGNATURES = {
     "b200ldl_symbolic_sizes": (ctypes.c_int, [_vp, _i32p, _i32p]),
     "b200ldl_get_symbolic": (ctypes.c_int, [_vp] + [_i32p] * 7),
     "b200ldl_node_pivots": (ctypes.c_int, [_vp, _i32p, _i32p]),
+    "b200ldl_get_pivot_record": (ctypes.c_int, [_vp, _i32p, _i32p, _i32p, _i32p,
+                                                ctypes.POINTER(ctypes.c_longlong)]),
+    "b200ldl_set_pivot_record": (ctypes.c_int, [_vp, _i32p, _i32p, _i32p, _i32p]),
+    "b200ldl_reuse_pivot_order": (ctypes.c_int, [_vp]),
     "b200ldl_stats": (ctypes.c_int, [_vp, _f64p, ctypes.c_int]),
     "b200ldl_set_profiling": (ctypes.c_int, [_vp, ctypes.c_int]),
     "b200ldl_reset_profile": (ctypes.c_int, [_vp]),

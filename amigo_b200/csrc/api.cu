@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -75,7 +76,10 @@ struct b200ldl_handle {
   cudaStream_t stream = nullptr;
   std::string last_error;
 
-  Symbolic sym;
+  // sym: the supernodal structure the factorization runs on; sym_ref: the
+  // reference's symbolic structure (the same until a pivot order is reused)
+  Symbolic sym, sym_ref;
+  bool replanned = false;
   bool uploaded = false;
   // independent systems factored as one forest (1 for a single system)
   int nsys = 1;
@@ -167,10 +171,14 @@ void build_plan(b200ldl_t h, const int* rowp, const int* cols) {
 
   // positions of the front variables of node k (own vars then contrib rows)
   std::vector<int> where(n, -1);
+  auto put = [&](int v, int pos) {
+    if (v < 0 || v >= n) throw std::runtime_error("front variable out of range");
+    if (pos >= 0 && where[v] >= 0) throw std::runtime_error("variable listed twice in one front");
+    where[v] = pos;
+  };
   auto mark = [&](int k, int sign) {
-    for (int j = 0; j < ns[k]; j++) where[s.node_to_var[s.node_ptr[k] + j]] = sign ? j : -1;
-    for (int t = 0; t < nc[k]; t++)
-      where[s.contrib_rows[s.contrib_ptr[k] + t]] = sign ? ns[k] + t : -1;
+    for (int j = 0; j < ns[k]; j++) put(s.node_to_var[s.node_ptr[k] + j], sign ? j : -1);
+    for (int t = 0; t < nc[k]; t++) put(s.contrib_rows[s.contrib_ptr[k] + t], sign ? ns[k] + t : -1);
   };
 
   std::vector<int> cmap(s.contrib_rows.size(), -1);
@@ -189,7 +197,8 @@ void build_plan(b200ldl_t h, const int* rowp, const int* cols) {
         const int i = cols[e];
         if (ip[i] < pj) continue;
         const int w = where[i];
-        if (w < 0) continue;
+        // an entry eliminated here must have its row in this front
+        if (w < 0) throw std::runtime_error("matrix entry outside the front that eliminates it");
         scat_csr.push_back(e);
         scat_row.push_back(w);
         scat_col.push_back(j);
@@ -295,6 +304,72 @@ void build_plan(b200ldl_t h, const int* rowp, const int* cols) {
   h->dcap = (unsigned long long)(dbl * g * 1.5) + (1u << 20);
 }
 
+// Supernodal structure from a pivot record: supernode k's pivot columns
+// become the variables it eliminated, in the order it eliminated them (a 2x2
+// pair stays adjacent), and the candidates it delayed join its contribution
+// rows ahead of the rows it already had. The elimination tree and the node
+// numbering are kept, so the permutation is the elimination order the record
+// describes. rec_f/rec_npiv/rec_ndel: per supernode; rec_fv: each
+// supernode's front variables after pivoting (f entries: pivots with 2x2
+// pairs encoded -(v+1), delayed, contribution rows), one after another.
+Symbolic replan_from_record(const Symbolic& tree, const int* rec_f, const int* rec_npiv,
+                            const int* rec_ndel, const int* rec_fv) {
+  const int n = tree.n, nn = tree.num_nodes;
+  Symbolic s;
+  s.n = n;
+  s.num_nodes = nn;
+  s.permuted = true;
+  s.children_ptr = tree.children_ptr;
+  s.children = tree.children;
+  s.parent = tree.parent;
+  s.node_ptr.assign(1, 0);
+  s.contrib_ptr.assign(1, 0);
+  s.node_to_var.reserve(n);
+  long long off = 0;
+  for (int k = 0; k < nn; k++) {
+    const int f = rec_f[k], np = rec_npiv[k], nd = rec_ndel[k];
+    if (f < 0 || np < 0 || nd < 0 || np + nd > f)
+      throw std::invalid_argument("pivot record: inconsistent front sizes");
+    const int* fv = rec_fv + off;
+    for (int t = 0; t < np; t++) {
+      const int v = fv[t] >= 0 ? fv[t] : -fv[t] - 1;
+      s.node_to_var.push_back(v);
+    }
+    for (int t = np; t < f; t++) s.contrib_rows.push_back(fv[t]);
+    s.node_ptr.push_back((int)s.node_to_var.size());
+    s.contrib_ptr.push_back((int)s.contrib_rows.size());
+    off += f;
+  }
+  if ((int)s.node_to_var.size() != n)
+    throw std::invalid_argument("pivot record: pivots do not cover every variable once");
+  s.iperm.assign(n, -1);
+  for (int q = 0; q < n; q++) {
+    const int v = s.node_to_var[q];
+    if (v < 0 || v >= n || s.iperm[v] >= 0)
+      throw std::invalid_argument("pivot record: pivots do not cover every variable once");
+    s.iperm[v] = q;
+  }
+  s.perm = s.node_to_var;
+  return s;
+}
+
+// Switch the handle to structure `s` (the device plan is rebuilt at the next
+// factorization; the last factor is dropped).
+void use_structure(b200ldl_t h, Symbolic&& s) {
+  Symbolic old = std::move(h->sym);
+  h->sym = std::move(s);
+  try {
+    build_plan(h, h->h_rowp.data(), h->h_cols.data());
+  } catch (...) {
+    h->sym = std::move(old);
+    build_plan(h, h->h_rowp.data(), h->h_cols.data());
+    throw;
+  }
+  h->uploaded = false;
+  h->factored = false;
+  h->fmax = 0;
+}
+
 void upload_plan(b200ldl_t h) {
   if (h->uploaded) return;
   const Symbolic& s = h->sym;
@@ -387,15 +462,26 @@ void ensure_pools(b200ldl_t h) {
   bind_state(h);
 }
 
+// Kernel attributes (shared memory sizes, cluster sizes) are set once per
+// device, on the device that is current, under a lock so that threads
+// driving different devices or handles do not race.
+void configure_device_kernels() {
+  static std::mutex mu;
+  static std::vector<char> done;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if ((int)done.size() > dev && done[dev]) return;
+  CK(configure_factor_kernels());
+  CK(configure_solve_kernels());
+  CK(configure_solve_big_kernels());
+  CK(configure_big_kernels());
+  if ((int)done.size() <= dev) done.resize(dev + 1, 0);
+  done[dev] = 1;
+}
+
 void run_factor(b200ldl_t h, const double* vals, const double* diag) {
-  static bool configured = false;
-  if (!configured) {
-    CK(configure_factor_kernels());
-    CK(configure_solve_kernels());
-    CK(configure_solve_big_kernels());
-    CK(configure_big_kernels());
-    configured = true;
-  }
+  configure_device_kernels();
   FactorParams prm{h->ustab, h->pivot_tol, h->solver_type == B200LDL_CHOLESKY ? 1 : 0};
   for (int attempt = 0; attempt < 12; attempt++) {
     ensure_pools(h);
@@ -874,6 +960,74 @@ int b200ldl_node_pivots(b200ldl_t h, int* num_pivots, int* num_delayed) {
     if (num_delayed) CK(cudaMemcpy(num_delayed, h->d_ndel.ptr, nn * sizeof(int), cudaMemcpyDeviceToHost));
     return 0;
   });
+}
+
+int b200ldl_get_pivot_record(b200ldl_t h, int* f, int* npiv, int* ndel, int* fv,
+                             long long* fv_len) {
+  return guarded(h, [&]() {
+    if (!h->factored) return fail(h, -5, "no factorization");
+    const int nn = h->sym.num_nodes;
+    std::vector<int> hf(nn), hp(nn), hd(nn);
+    std::vector<int64_t> ho(nn);
+    if (nn > 0) {
+      CK(cudaMemcpy(hf.data(), h->d_f.ptr, nn * sizeof(int), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(hp.data(), h->d_npiv.ptr, nn * sizeof(int), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(hd.data(), h->d_ndel.ptr, nn * sizeof(int), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(ho.data(), h->d_fv_off.ptr, nn * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    }
+    long long total = 0;
+    for (int k = 0; k < nn; k++) total += hf[k];
+    if (fv_len) *fv_len = total;
+    if (f) std::copy(hf.begin(), hf.end(), f);
+    if (npiv) std::copy(hp.begin(), hp.end(), npiv);
+    if (ndel) std::copy(hd.begin(), hd.end(), ndel);
+    if (fv && total > 0) {
+      std::vector<int> pool(h->used[0]);
+      CK(cudaMemcpy(pool.data(), h->d_ivars.ptr, pool.size() * sizeof(int),
+                    cudaMemcpyDeviceToHost));
+      long long o = 0;
+      for (int k = 0; k < nn; k++) {
+        if (ho[k] < 0 || (unsigned long long)(ho[k] + hf[k]) > h->used[0])
+          return fail(h, -4, "front variables of supernode %d outside the used pool", k);
+        std::copy(pool.begin() + ho[k], pool.begin() + ho[k] + hf[k], fv + o);
+        o += hf[k];
+      }
+    }
+    return 0;
+  });
+}
+
+int b200ldl_set_pivot_record(b200ldl_t h, const int* f, const int* npiv, const int* ndel,
+                             const int* fv) {
+  return guarded(h, [&]() {
+    if (h->solver_type == B200LDL_CHOLESKY) return fail(h, -1, "Cholesky mode has no pivot order");
+    if (!f && !npiv && !ndel && !fv) {
+      if (h->replanned) {
+        use_structure(h, Symbolic(h->sym_ref));
+        h->replanned = false;
+      }
+      return 0;
+    }
+    if (!f || !npiv || !ndel || !fv) return fail(h, -1, "incomplete pivot record");
+    if (!h->replanned) h->sym_ref = h->sym;
+    Symbolic s = replan_from_record(h->sym_ref, f, npiv, ndel, fv);
+    use_structure(h, std::move(s));
+    h->replanned = true;
+    return 0;
+  });
+}
+
+int b200ldl_reuse_pivot_order(b200ldl_t h) {
+  if (!h) return -1;
+  const int nn = h->sym.num_nodes;
+  long long total = 0;
+  int st = b200ldl_get_pivot_record(h, nullptr, nullptr, nullptr, nullptr, &total);
+  if (st != 0) return st;
+  std::vector<int> f(std::max(1, nn)), np(std::max(1, nn)), nd(std::max(1, nn));
+  std::vector<int> fv(std::max<long long>(1, total));
+  st = b200ldl_get_pivot_record(h, f.data(), np.data(), nd.data(), fv.data(), &total);
+  if (st != 0) return st;
+  return b200ldl_set_pivot_record(h, f.data(), np.data(), nd.data(), fv.data());
 }
 
 int b200ldl_stats(b200ldl_t h, double* stats, int nstats) {

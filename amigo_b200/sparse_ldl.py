@@ -394,8 +394,48 @@ class SparseLDL:
         _native.check(self._h, st, "node_pivots")
         return a, b
 
+    # -- pivot-order reuse --------------------------------------------------------
+    def pivot_record(self) -> dict:
+        """The last factorization's pivot record: per supernode the front size
+        ``f``, pivots ``npiv`` and delayed candidates ``ndel``, and ``fv``,
+        each front's variables after pivoting (pivots in elimination order
+        with 2x2 pairs encoded -(v+1), delayed, contribution rows)."""
+        nn = len(self.symbolic()["node_ptr"]) - 1
+        total = ctypes.c_longlong()
+        st = self._lib.b200ldl_get_pivot_record(self._h, None, None, None, None,
+                                                ctypes.byref(total))
+        _native.check(self._h, st, "get_pivot_record")
+        rec = {k: np.empty(max(nn, 1), np.int32) for k in ("f", "npiv", "ndel")}
+        rec["fv"] = np.empty(max(total.value, 1), np.int32)
+        st = self._lib.b200ldl_get_pivot_record(
+            self._h, *[rec[k].ctypes.data_as(_native._i32p) for k in ("f", "npiv", "ndel", "fv")],
+            ctypes.byref(total))
+        _native.check(self._h, st, "get_pivot_record")
+        return {"f": rec["f"][:nn], "npiv": rec["npiv"][:nn], "ndel": rec["ndel"][:nn],
+                "fv": rec["fv"][:total.value]}
+
+    def set_pivot_record(self, rec=None):
+        """Re-plan the fronts from a pivot record (``pivot_record()`` of any
+        factorization of this pattern): each candidate is then tested first
+        in the front that accepted it. ``None`` returns to the reference's
+        symbolic structure. Factor again before solving."""
+        if rec is None:
+            st = self._lib.b200ldl_set_pivot_record(self._h, None, None, None, None)
+        else:
+            arrs = [np.ascontiguousarray(rec[k], np.int32) for k in ("f", "npiv", "ndel", "fv")]
+            st = self._lib.b200ldl_set_pivot_record(
+                self._h, *[a.ctypes.data_as(_native._i32p) for a in arrs])
+        _native.check(self._h, st, "set_pivot_record")
+
+    def reuse_pivot_order(self):
+        """Re-plan the fronts from the last factorization's own pivot record
+        (the pattern's next factorizations, e.g. the next interior-point
+        iterations, then test each candidate where it was accepted)."""
+        st = self._lib.b200ldl_reuse_pivot_order(self._h)
+        _native.check(self._h, st, "reuse_pivot_order")
+
     # -- profiling ---------------------------------------------------------------
-    PHASES = ("fronts", "big_assembly", "big_panel", "big_update", "solve_forward",
+    PHASES =("fronts", "big_assembly", "big_panel", "big_update", "solve_forward",
               "solve_backward", "cluster_fronts")
 
     def set_profiling(self, on: bool):

@@ -165,7 +165,9 @@ const char* b200ldl_last_error(b200ldl_t h);
  * of contribution rows. */
 int b200ldl_symbolic_sizes(b200ldl_t h, int* num_nodes, int* num_contrib);
 
-/* Copy the symbolic structure to host arrays (any pointer may be NULL):
+/* Copy the supernodal structure the factorizations run on (the reference's
+ * symbolic structure unless b200ldl_set_pivot_record replaced it) to host
+ * arrays (any pointer may be NULL):
  * invperm [n], node_ptr [num_nodes+1], node_to_var [n], children_ptr
  * [num_nodes+2] (roots in slot num_nodes), children [num_nodes],
  * contrib_ptr [num_nodes+1], contrib_rows [num_contrib]. Same layout and
@@ -178,6 +180,39 @@ int b200ldl_get_symbolic(b200ldl_t h, int* invperm, int* node_ptr,
 /* Per-supernode pivot and delayed-pivot counts of the last factorization
  * (host arrays of length num_nodes). */
 int b200ldl_node_pivots(b200ldl_t h, int* num_pivots, int* num_delayed);
+
+/* Pivot-order reuse (no counterpart in the reference: every
+ * SparseLDL::factor starts again from the symbolic supernodes,
+ * include/sparse_ldl.h:136-158, and delays the same candidates through the
+ * same fronts each time, factor_front_matrix_block, sparse_ldl.h:1316-1553).
+ *
+ * The pivot record of a factorization is, per supernode k, its front size
+ * f[k], its pivots npiv[k], its delayed candidates ndel[k], and its front
+ * variables after pivoting: npiv[k] pivots in elimination order (2x2 pairs
+ * adjacent, each encoded -(v+1)), then the ndel[k] delayed candidates, then
+ * the contribution rows; fv holds these lists one supernode after another
+ * (sum of f[k] entries). b200ldl_get_pivot_record reads it from the last
+ * factorization into host arrays (any may be NULL; *fv_len receives the
+ * length of fv). */
+int b200ldl_get_pivot_record(b200ldl_t h, int* f, int* npiv, int* ndel, int* fv,
+                             long long* fv_len);
+
+/* Re-plan the fronts from a pivot record (host arrays as above, num_nodes
+ * entries each, from any factorization of this pattern): supernode k's
+ * pivot columns become the variables it eliminated, in that order, and the
+ * candidates it delayed become contribution rows, so each candidate is
+ * tested in the front that accepted it instead of being delayed through the
+ * fronts below it. The elimination tree is kept; the threshold tests and
+ * delays still apply to every factorization, so a candidate that fails in
+ * its new front is delayed as before. All four pointers NULL returns to the
+ * reference's symbolic structure. The last factor is dropped; factor again
+ * before solving. Status -4 if the record does not describe a valid
+ * elimination of this pattern (the handle keeps its structure). */
+int b200ldl_set_pivot_record(b200ldl_t h, const int* f, const int* npiv, const int* ndel,
+                             const int* fv);
+
+/* b200ldl_set_pivot_record with the last factorization's own record. */
+int b200ldl_reuse_pivot_order(b200ldl_t h);
 
 /* Statistics of the last factorization: stats[0] = factor flops actually
  * executed (dense partial factorizations of the fronts as sized at run

@@ -393,3 +393,21 @@ void ldlo_solve(ldlo* h, int nrhs, double* x, int ldx) {
   }
   free(t);
 }
+
+/* Pivot record of the last factorization (test access): per supernode the
+ * front size, pivots and delayed candidates, and the front variables after
+ * pivoting (pivots in elimination order with 2x2 pairs encoded -(v+1), then
+ * the delayed candidates, then the contribution rows) one supernode after
+ * another. Any pointer may be NULL; returns the length of fv. */
+long long ldlo_pivot_record(ldlo* h, int* f, int* npiv, int* ndel, int* fv) {
+  long long o = 0;
+  for (int k = 0; k < h->nn; k++) {
+    if (f) f[k] = h->f[k];
+    if (npiv) npiv[k] = h->npiv[k];
+    if (ndel) ndel[k] = h->ndel[k];
+    if (fv)
+      for (int t = 0; t < h->f[k]; t++) fv[o + t] = h->fv[k][t];
+    o += h->f[k];
+  }
+  return o;
+}

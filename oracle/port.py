@@ -31,6 +31,8 @@ def load():
         lib.ldlo_factor.argtypes = [ctypes.c_void_p, _f64p, _f64p]
         lib.ldlo_solve.argtypes = [ctypes.c_void_p, ctypes.c_int, _f64p, ctypes.c_int]
         lib.ldlo_inertia.argtypes = [ctypes.c_void_p, _i32p, _i32p]
+        lib.ldlo_pivot_record.restype = ctypes.c_longlong
+        lib.ldlo_pivot_record.argtypes = [ctypes.c_void_p, _i32p, _i32p, _i32p, _i32p]
         _lib = lib
     return _lib
 
@@ -73,6 +75,19 @@ class PortLDL:
         nrhs = 1 if x.ndim == 1 else x.shape[1]
         self._lib.ldlo_solve(self._h, nrhs, x.ctypes.data_as(_f64p), self.n)
         return x
+
+    def pivot_record(self) -> dict:
+        """Per supernode: front size, pivots, delayed candidates, and the
+        front variables after pivoting, in the layout of
+        ``amigo_b200.sparse_ldl.SparseLDL.pivot_record``."""
+        nn = len(self._sym["node_ptr"]) - 1
+        total = self._lib.ldlo_pivot_record(self._h, None, None, None, None)
+        rec = {k: np.empty(max(nn, 1), np.int32) for k in ("f", "npiv", "ndel")}
+        rec["fv"] = np.empty(max(total, 1), np.int32)
+        self._lib.ldlo_pivot_record(self._h, *[rec[k].ctypes.data_as(_i32p)
+                                               for k in ("f", "npiv", "ndel", "fv")])
+        return {"f": rec["f"][:nn], "npiv": rec["npiv"][:nn], "ndel": rec["ndel"][:nn],
+                "fv": rec["fv"][:total]}
 
     def inertia(self):
         p = ctypes.c_int()

@@ -2,7 +2,7 @@
 
 Runs in the build container only (it reads the reference sources):
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py <reference checkout>
 
 1. Executes ``get_matrix`` and ``get_poisson_2d`` from the reference's
    tests/unit/test_ldl.py (with the compiled ``amigo`` module replaced by a
@@ -48,7 +48,7 @@ def _load_reference_helpers(ref_root: str):
     return ns["get_matrix"], ns["get_poisson_2d"]
 
 
-def main(ref_root: str = "/root/reference") -> None:
+def main(ref_root: str) -> None:
     from oracle import ref
 
     get_matrix, get_poisson_2d = _load_reference_helpers(ref_root)
@@ -84,4 +84,6 @@ def main(ref_root: str = "/root/reference") -> None:
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference checkout>")
+    main(sys.argv[1])

@@ -37,7 +37,9 @@ def load_reference(ref_root):
 
 
 def main(argv):
-    ref_root = argv[1] if len(argv) > 1 else "/root/reference"
+    if len(argv) != 2:
+        sys.exit("usage: python tests/golden/make_inertia_golden.py <reference checkout>")
+    ref_root = argv[1]
     cls = load_reference(ref_root)
     out = {}
     for name, systems in scenarios().items():
