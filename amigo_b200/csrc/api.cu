@@ -424,8 +424,8 @@ void upload_plan(b200ldl_t h) {
   CK(h->d_flops.alloc(kWork));
   CK(h->d_used.alloc(3));
   CK(h->d_big.alloc(nn));
-  CK(h->d_big_meta.alloc(16));
-  CK(h->d_class_list.alloc((size_t)6 * std::max(1, nn)));
+  CK(h->d_big_meta.alloc(kBigMeta));
+  CK(h->d_class_list.alloc((size_t)7 * std::max(1, nn)));
   h->uploaded = true;
 }
 
@@ -482,7 +482,11 @@ void configure_device_kernels() {
 
 void run_factor(b200ldl_t h, const double* vals, const double* diag) {
   configure_device_kernels();
-  FactorParams prm{h->ustab, h->pivot_tol, h->solver_type == B200LDL_CHOLESKY ? 1 : 0};
+  // fronts re-planned from a pivot record are expected to accept their
+  // candidates where they stand: their big fronts take the blocked panels
+  // with a-posteriori tests
+  FactorParams prm{h->ustab, h->pivot_tol, h->solver_type == B200LDL_CHOLESKY ? 1 : 0,
+                   (h->replanned && h->solver_type != B200LDL_CHOLESKY) ? 1 : 0};
   for (int attempt = 0; attempt < 12; attempt++) {
     ensure_pools(h);
     CK(cudaMemsetAsync(h->d_used.ptr, 0, 3 * sizeof(unsigned long long), h->stream));
@@ -496,15 +500,15 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
       const int b = h->level_ptr[l];
       const int cnt = h->level_ptr[l + 1] - b;
       if (h->level_may_big[l])
-        CK(cudaMemsetAsync(h->d_big_meta.ptr, 0, 16 * sizeof(int), h->stream));
+        CK(cudaMemsetAsync(h->d_big_meta.ptr, 0, kBigMeta * sizeof(int), h->stream));
       h->prof.begin(h->stream);
       launch_factor_level(h->plan, h->st, h->d_level_nodes.ptr + b, cnt, prm, h->stream,
                           vals, diag);
       h->prof.end(kPhFront, h->stream, 1);
       CK(cudaGetLastError());
       if (!h->level_may_big[l]) continue;
-      int meta[16];
-      CK(cudaMemcpyAsync(meta, h->d_big_meta.ptr, 16 * sizeof(int), cudaMemcpyDeviceToHost,
+      int meta[kBigMeta];
+      CK(cudaMemcpyAsync(meta, h->d_big_meta.ptr, kBigMeta * sizeof(int), cudaMemcpyDeviceToHost,
                          h->stream));
       CK(cudaStreamSynchronize(h->stream));
       if (meta[0] > 0) {
@@ -515,6 +519,9 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
         info.count_large = meta[3];
         info.max_fs_large = meta[4];
         info.max_f_large = meta[15];
+        info.count_app = meta[16];
+        info.max_f_app = meta[17];
+        info.max_fs_app = meta[18];
         info.cluster_launches = 0;
         for (int c = 0; c < 5; c++) {
           info.class_count[c] = meta[5 + c];

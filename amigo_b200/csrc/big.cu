@@ -781,6 +781,70 @@ cudaError_t launch_panel(const DevState& s, const FactorParams& prm, int count, 
 
 constexpr size_t kPanelSmemMax = 224 * 1024;
 
+void assemble_big(const DevPlan& p, const DevState& s, const int* list, int nl, int max_f,
+                  int maxkids, const double* vals, const double* diag, cudaStream_t stream,
+                  Prof& prof) {
+  const int ych = std::min(256, (max_f + 7) / 8);
+  prof.begin(stream);
+  big_zero_kernel<<<dim3(nl, ych), 256, 0, stream>>>(s, list);
+  big_scatter_kernel<<<dim3(nl, 16), 256, 0, stream>>>(p, s, vals, diag, list);
+  if (diag) big_diag_kernel<<<nl, 256, 0, stream>>>(p, s, diag, list);
+  for (int c = 0; c < maxkids; c++)
+    big_extend_kernel<<<dim3(nl, ych), 256, 0, stream>>>(p, s, c, list);
+  prof.end(kPhBigAsm, stream, 2 + (diag ? 1 : 0) + maxkids);
+}
+
+void update_big(const DevState& s, const int* list, int count, cudaStream_t stream, Prof& prof) {
+  const int upd_grid = 148 * 4;
+  prof.begin(stream);
+  for (int c0 = 0; c0 < count; c0 += kUpdMaxFronts) {
+    const int nl = std::min(kUpdMaxFronts, count - c0);
+    big_update_kernel<<<upd_grid, kUpdThreads, 0, stream>>>(s, list + c0, nl);
+  }
+  prof.end(kPhBigUpd, stream, (count + kUpdMaxFronts - 1) / kUpdMaxFronts);
+}
+
+// Class-6 fronts: blocked panels with a-posteriori tests (big_app.cu). The
+// steps a level needs without failed tests are launched back to back; then
+// the fronts still open (a failed test delays a candidate and shortens its
+// panel) are counted on the device and the loop continues until none is.
+cudaError_t app_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
+                      int maxkids, const FactorParams& prm, const double* vals,
+                      const double* diag, cudaStream_t stream, Prof& prof) {
+  const int nl = info.count_app;
+  const int* list6 = s.class_list + (size_t)6 * p.num_nodes;
+  assemble_big(p, s, list6, nl, info.max_f_app, maxkids, vals, diag, stream, prof);
+  int step = 1;
+  int nsteps = (info.max_fs_app + kBigPanelMax - 1) / kBigPanelMax + 1;
+  for (int round = 0;; round++) {
+    for (int t = 0; t < nsteps; t++, step++) {
+      prof.begin(stream);
+      cudaError_t e = launch_app_panel(s, prm, nl, info.max_f_app, list6, step, stream);
+      if (e != cudaSuccess) return e;
+      prof.end(kPhBigPanel, stream, 3);
+      update_big(s, list6, nl, stream, prof);
+      prof.begin(stream);
+      e = launch_app_delay(s, nl, list6, step, stream);
+      if (e != cudaSuccess) return e;
+      prof.end(kPhBigPanel, stream, 1);
+    }
+    cudaError_t e = cudaMemsetAsync(s.big_meta + 19, 0, 2 * sizeof(int), stream);
+    if (e != cudaSuccess) return e;
+    e = launch_app_open_count(s, nl, list6, stream);
+    if (e != cudaSuccess) return e;
+    int open[2] = {0, 0};
+    e = cudaMemcpyAsync(open, s.big_meta + 19, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return e;
+    if (open[0] == 0) break;
+    // every step accepts a pivot or delays a candidate, so this ends
+    nsteps = (open[1] + kBigPanelMax - 1) / kBigPanelMax + 1;
+    if (round > 4 * (info.max_fs_app + 1)) return cudaErrorUnknown;
+  }
+  return cudaSuccess;
+}
+
 }  // namespace
 
 cudaError_t configure_big_kernels() {
@@ -815,6 +879,10 @@ cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevel
     if (e != cudaSuccess) return e;
   }
   prof.end(kPhCluster, stream, info.cluster_launches);
+  if (info.count_app > 0) {
+    cudaError_t e = app_level(p, s, info, maxkids, prm, vals, diag, stream, prof);
+    if (e != cudaSuccess) return e;
+  }
   if (info.count_large == 0) {
     prof.begin(stream);
     big_finalize_kernel<<<(nb + 255) / 256, 256, 0, stream>>>(s, nb, prm.cholesky);

@@ -156,7 +156,9 @@ __global__ void __launch_bounds__(kFactorThreads)
       // on-chip limit also get the chained panel's W by physical row and its
       // permutation scratch
       unsigned long long need = (unsigned long long)f * f + (unsigned long long)kBigPanelMax * f;
-      if (f > s.cf_limit[4])
+      if (prm.app && nc > 0)
+        need += (unsigned long long)kAppScratch;
+      else if (f > s.cf_limit[4])
         need += (unsigned long long)kBigPanelMax * f + (unsigned long long)(fs + 1) * f;
       const unsigned long long dofs = atomicAdd(s.used + 1, need);
       if (dofs + need > s.dcap) fail = 1;
@@ -192,10 +194,20 @@ __global__ void __launch_bounds__(kFactorThreads)
       const int slot = atomicAdd(s.big_meta, 1);
       atomicMax(s.big_meta + 1, f);
       atomicMax(s.big_meta + 2, fs);
+      const bool app = prm.app && nc > 0;
       int cls = 5;
-      for (int c = 4; c >= 0; c--)
-        if (f <= s.cf_limit[c]) cls = c;
-      if (cls == 5) {
+      if (app) {
+        cls = 6;
+      } else {
+        for (int c = 4; c >= 0; c--)
+          if (f <= s.cf_limit[c]) cls = c;
+      }
+      if (cls == 6) {
+        const int q = atomicAdd(s.big_meta + 16, 1);
+        atomicMax(s.big_meta + 17, f);
+        atomicMax(s.big_meta + 18, fs);
+        s.class_list[(size_t)6 * p.num_nodes + q] = slot;
+      } else if (cls == 5) {
         const int q = atomicAdd(s.big_meta + 3, 1);
         atomicMax(s.big_meta + 4, fs);
         atomicMax(s.big_meta + 15, f);
@@ -220,9 +232,12 @@ __global__ void __launch_bounds__(kFactorThreads)
       b.npos = 0;
       b.nneg = 0;
       b.pad = 0;
+      b.app = app ? 1 : 0;
+      b.pending = -1;
       b.ioff = sh_ioff;
       b.doff = sh_doff;
       b.woff = sh_doff + (long long)f * f;
+      b.xoff = b.woff + (long long)kBigPanelMax * f;
       b.flops = 0.0;
       s.big[slot] = b;
     }

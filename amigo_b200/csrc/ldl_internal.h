@@ -109,13 +109,20 @@ struct BigFront {
   int state;  // 0 active, 1 finished after the pending update, 2 done
   int npos, nneg;
   int pad;
+  int app;      // 1: blocked panels with a-posteriori threshold tests (big_app.cu)
+  int pending;  // a-posteriori panels: candidate position to delay after the update, or -1
   long long ioff;  // front variables (fv[f], orig[f]) in the int pool
   long long doff;  // the front F (f x f, column-major) in the double pool
   long long woff;  // the panel's W columns (f x kBigPanelMax) in the double pool
+  long long xoff;  // a-posteriori panels: the diagonal block's factor and tests
   double flops;
 };
 
 constexpr int kBigPanelMax = 32;
+// doubles of per-front scratch for the a-posteriori panels (big_app.cu)
+constexpr int kAppScratch = 1536;
+// ints of big-front level metadata (factor.cu fills, the host reads back)
+constexpr int kBigMeta = 24;
 
 // Mutable state of one factorization (device memory).
 struct DevState {
@@ -140,9 +147,11 @@ struct DevState {
                     // [2] big trailing updates, [3] trailing-update bytes
                     // moved, [4] fronts factored on chip in a cluster
   BigFront* big;    // [nn] big fronts of the current level
-  int* big_meta;    // [16]: count, max f, max fs, count large, max fs large,
-                    // class counts [5..9], class max f [10..14]
-  int* class_list;  // [6][nn] big-front indices per size class
+  int* big_meta;    // [kBigMeta]: count, max f, max fs, count large, max fs
+                    // large, class counts [5..9], class max f [10..14], max f
+                    // large [15], a-posteriori fronts: count [16], max f [17],
+                    // max fs [18], not yet done [19], most candidates left [20]
+  int* class_list;  // [7][nn] big-front indices per size class (6: a-posteriori)
   int cf_limit[5];  // largest front of each on-chip class
 };
 
@@ -150,6 +159,10 @@ struct FactorParams {
   double ustab;
   double pivot_tol;
   int cholesky;
+  // fronts above the shared-memory limit that have contribution rows are
+  // factored in blocked panels with a-posteriori threshold tests
+  // (big_app.cu) instead of the candidate-by-candidate search
+  int app;
 };
 
 // Largest front factored entirely in shared memory (fp64, ld = f | 1).
@@ -171,6 +184,7 @@ struct BigLevelInfo {
   int class_count[5], class_maxf[5];
   int cluster_launches;
   int max_f_large;  // largest front of class 5
+  int count_app, max_f_app, max_fs_app;  // class 6: a-posteriori panels
 };
 
 // Fronts above kSmemFrontMax are factored on chip by a cluster of 1, 2, 4,
@@ -190,6 +204,20 @@ int big_chain_panel_width(int f);
 cudaError_t configure_big_chain_kernel();
 cudaError_t launch_big_chain_panel(const DevState& s, const FactorParams& prm, int count,
                                    int max_f, int nb, const int* list, cudaStream_t stream);
+
+// A-posteriori blocked panels (big_app.cu) for the class-6 fronts in
+// `list`: one panel step (diagonal block, rows below and tests, accepted
+// columns), and the delay of a candidate whose test failed (after the
+// trailing update of the step). `step` numbers the steps of one level from 1
+// up; the panel state is stamped with it.
+cudaError_t launch_app_panel(const DevState& s, const FactorParams& prm, int count, int max_f,
+                             const int* list, int step, cudaStream_t stream);
+cudaError_t launch_app_delay(const DevState& s, int count, const int* list, int step,
+                             cudaStream_t stream);
+// number of class-6 fronts not yet done into s.big_meta[19], the most
+// candidates any of them has left into s.big_meta[20]
+cudaError_t launch_app_open_count(const DevState& s, int count, const int* list,
+                                  cudaStream_t stream);
 
 cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
                              int maxkids, const FactorParams& prm, const double* vals,
