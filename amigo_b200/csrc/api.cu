@@ -80,6 +80,9 @@ struct b200ldl_handle {
   // reference's symbolic structure (the same until a pivot order is reused)
   Symbolic sym, sym_ref;
   bool replanned = false;
+  // 2x2 partners of the pivot record the structure was re-planned from
+  std::vector<int> partner;
+  DevBuf<int> d_partner;
   bool uploaded = false;
   // independent systems factored as one forest (1 for a single system)
   int nsys = 1;
@@ -313,7 +316,7 @@ void build_plan(b200ldl_t h, const int* rowp, const int* cols) {
 // supernode's front variables after pivoting (f entries: pivots with 2x2
 // pairs encoded -(v+1), delayed, contribution rows), one after another.
 Symbolic replan_from_record(const Symbolic& tree, const int* rec_f, const int* rec_npiv,
-                            const int* rec_ndel, const int* rec_fv) {
+                            const int* rec_ndel, const int* rec_fv, std::vector<int>& partner) {
   const int n = tree.n, nn = tree.num_nodes;
   Symbolic s;
   s.n = n;
@@ -334,6 +337,19 @@ Symbolic replan_from_record(const Symbolic& tree, const int* rec_f, const int* r
     for (int t = 0; t < np; t++) {
       const int v = fv[t] >= 0 ? fv[t] : -fv[t] - 1;
       s.node_to_var.push_back(v);
+    }
+    // 2x2 pivots are consecutive pairs of encoded entries
+    for (int t = 0; t < np;) {
+      if (fv[t] < 0 && t + 1 < np && fv[t + 1] < 0) {
+        const int a = -fv[t] - 1, b = -fv[t + 1] - 1;
+        if (a >= 0 && a < n && b >= 0 && b < n) {
+          partner[a] = b;
+          partner[b] = a;
+        }
+        t += 2;
+      } else {
+        t += 1;
+      }
     }
     for (int t = np; t < f; t++) s.contrib_rows.push_back(fv[t]);
     s.node_ptr.push_back((int)s.node_to_var.size());
@@ -390,6 +406,7 @@ void upload_plan(b200ldl_t h) {
   CK(h->d_level_nodes.upload(h->hp_level_nodes));
   CK(h->d_rowp.upload(h->h_rowp));
   CK(h->d_cols.upload(h->h_cols));
+  if (h->replanned) CK(h->d_partner.upload(h->partner));
 
   DevPlan& p = h->plan;
   p.n = s.n;
@@ -453,6 +470,7 @@ void bind_state(b200ldl_t h) {
   st.big_meta = h->d_big_meta.ptr;
   st.class_list = h->d_class_list.ptr;
   for (int c = 0; c < 5; c++) st.cf_limit[c] = cluster_front_limit(c);
+  st.partner = h->replanned ? h->d_partner.ptr : nullptr;
 }
 
 void ensure_pools(b200ldl_t h) {
@@ -1017,8 +1035,10 @@ int b200ldl_set_pivot_record(b200ldl_t h, const int* f, const int* npiv, const i
     }
     if (!f || !npiv || !ndel || !fv) return fail(h, -1, "incomplete pivot record");
     if (!h->replanned) h->sym_ref = h->sym;
-    Symbolic s = replan_from_record(h->sym_ref, f, npiv, ndel, fv);
+    std::vector<int> partner(std::max(1, h->n), -1);
+    Symbolic s = replan_from_record(h->sym_ref, f, npiv, ndel, fv, partner);
     use_structure(h, std::move(s));
+    h->partner = std::move(partner);
     h->replanned = true;
     return 0;
   });

@@ -99,6 +99,9 @@ __global__ void big_zero_kernel(DevState s, const int* __restrict__ list) {
     double* col = F + (size_t)f * j;
     for (int i = j + lane; i < f; i += 32) col[i] = 0.0;
   }
+  // a-posteriori panels: no column maxima for the first panel yet
+  if (B.app && blockIdx.y == 0 && threadIdx.x < kBigPanelMax)
+    s.dpool[B.xoff + kAppNextColmax + threadIdx.x] = 0.0;
 }
 
 __global__ void big_scatter_kernel(DevPlan p, DevState s, const double* __restrict__ vals,
@@ -705,6 +708,27 @@ __global__ void __launch_bounds__(kUpdThreads, 2)
       for (int a = 0; a < 4; a++) {
         const int i = i0 + tx + 16 * a;
         if (i < f && i >= j) F[i + (size_t)f * j] = cur[a][b] - acc[a][b];
+      }
+    }
+    if (B.app && J == 0) {
+      // the next panel's columns [k, k + 32): their largest magnitude over
+      // the rows below the next block, for its diagonal-block tests (the
+      // 16 threads with the same ty are one half-warp)
+      unsigned long long* nxt =
+          reinterpret_cast<unsigned long long*>(s.dpool + B.xoff + kAppNextColmax);
+#pragma unroll
+      for (int b = 0; b < 2; b++) {
+        double m = 0.0;
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+          const int i = i0 + tx + 16 * a;
+          if (i < f && i >= k + kBigPanelMax) m = fmax(m, fabs(cur[a][b] - acc[a][b]));
+        }
+#pragma unroll
+        for (int o = 1; o < 16; o <<= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        const int j = j0 + ty + 16 * b;
+        if (tx == 0 && j < f && m > 0.0)
+          atomicMax(nxt + (ty + 16 * b), (unsigned long long)__double_as_longlong(m));
       }
     }
   }

@@ -10,7 +10,7 @@
 namespace b200ldl {
 
 // Work counters accumulated on the device per factorization.
-constexpr int kWork = 5;
+constexpr int kWork = 8;
 
 // Kernel classes timed by the optional profiler.
 enum ProfPhase : int {
@@ -121,6 +121,10 @@ struct BigFront {
 constexpr int kBigPanelMax = 32;
 // doubles of per-front scratch for the a-posteriori panels (big_app.cu)
 constexpr int kAppScratch = 1536;
+// its first kBigPanelMax doubles: the largest magnitude in each of the next
+// panel's columns over the rows below its block, left there (as the bits of
+// non-negative doubles) by the trailing update of the previous panel
+constexpr int kAppNextColmax = 0;
 // ints of big-front level metadata (factor.cu fills, the host reads back)
 constexpr int kBigMeta = 24;
 
@@ -144,6 +148,9 @@ struct DevState {
                     // [2] completion ticket of the trailing-update launch
   int* inertia;     // [2] pos, neg
   double* flops;    // [kWork] executed flops: [0] all fronts, [1] big panels,
+                    // (a-posteriori panels: [5] panels, [6] pivots rejected by
+                    // the a-posteriori tests, [7] candidates delayed in the
+                    // diagonal block)
                     // [2] big trailing updates, [3] trailing-update bytes
                     // moved, [4] fronts factored on chip in a cluster
   BigFront* big;    // [nn] big fronts of the current level
@@ -153,6 +160,10 @@ struct DevState {
                     // max fs [18], not yet done [19], most candidates left [20]
   int* class_list;  // [7][nn] big-front indices per size class (6: a-posteriori)
   int cf_limit[5];  // largest front of each on-chip class
+  // fronts re-planned from a pivot record: partner[v] = the variable that
+  // formed a 2x2 pivot with v in the record, -1 otherwise (nullptr without a
+  // record)
+  const int* partner;
 };
 
 struct FactorParams {

@@ -448,10 +448,11 @@ class SparseLDL:
         return int(self._lib.b200ldl_launch_count(self._h))
 
     def work(self) -> dict:
-        v = np.zeros(5)
-        self._lib.b200ldl_work(self._h, v.ctypes.data_as(_native._f64p), 5)
+        v = np.zeros(8)
+        self._lib.b200ldl_work(self._h, v.ctypes.data_as(_native._f64p), 8)
         return {"flops": v[0], "panel_flops": v[1], "update_flops": v[2], "update_bytes": v[3],
-                "cluster_flops": v[4]}
+                "cluster_flops": v[4], "app_panels": int(v[5]), "app_rejected": int(v[6]),
+                "app_block_delays": int(v[7])}
 
     def profile(self) -> list:
         """Per kernel class: device milliseconds (CUDA events), launches, and

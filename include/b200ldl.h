@@ -238,7 +238,10 @@ long long b200ldl_launch_count(b200ldl_t h);
 /* Work of the last factorization: out[0] = flops executed in all fronts,
  * out[1] = of which in big-front panels, out[2] = in big-front trailing
  * updates, out[3] = bytes moved by the trailing updates, out[4] = flops in
- * fronts factored on chip in a thread-block cluster. */
+ * fronts factored on chip in a thread-block cluster; after pivot-order
+ * reuse, the blocked panels with a-posteriori tests: out[5] = panels,
+ * out[6] = panels cut short because the a-posteriori test rejected a pivot,
+ * out[7] = candidates delayed inside a panel's diagonal block. */
 int b200ldl_work(b200ldl_t h, double* out, int n);
 
 /* KKT assembly: element Hessian blocks into the values of the fixed CSR
@@ -300,7 +303,11 @@ void b200ldl_assembly_destroy(b200ldl_assembly_t a);
  * holds the array (2 MiB) until exit, all calls share it, and calls whose
  * kernels overlap on the GPU race on it (order them on one stream). The
  * first call on a device looks up the array's address; make it before any
- * stream capture. Calls no cudaMalloc/cudaFree or allocating routine. */
+ * stream capture. Calls no cudaMalloc/cudaFree or allocating routine.
+ * A singular matrix is not an error: a zero pivot (a column that is zero at
+ * its elimination) counts as positive in the inertia, as the reference
+ * counts it, and the solution component it divides gets 0; the status is
+ * still 0, so npos + nneg == n does not rule out singularity. */
 int b200ldl_dense_solve_noalloc(int n, const double* a, int lda, double* b,
                                 int ldb, int nrhs, int* inertia, void* stream);
 
