@@ -494,6 +494,7 @@ void configure_device_kernels() {
   CK(configure_solve_kernels());
   CK(configure_solve_big_kernels());
   CK(configure_big_kernels());
+  CK(configure_app_kernels());
   if ((int)done.size() <= dev) done.resize(dev + 1, 0);
   done[dev] = 1;
 }
@@ -504,7 +505,7 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
   // candidates where they stand: their big fronts take the blocked panels
   // with a-posteriori tests
   FactorParams prm{h->ustab, h->pivot_tol, h->solver_type == B200LDL_CHOLESKY ? 1 : 0,
-                   (h->replanned && h->solver_type != B200LDL_CHOLESKY) ? 1 : 0};
+                   (h->replanned && h->solver_type != B200LDL_CHOLESKY) ? 1 : 0, 0};
   for (int attempt = 0; attempt < 12; attempt++) {
     ensure_pools(h);
     CK(cudaMemsetAsync(h->d_used.ptr, 0, 3 * sizeof(unsigned long long), h->stream));

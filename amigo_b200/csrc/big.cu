@@ -710,27 +710,6 @@ __global__ void __launch_bounds__(kUpdThreads, 2)
         if (i < f && i >= j) F[i + (size_t)f * j] = cur[a][b] - acc[a][b];
       }
     }
-    if (B.app && J == 0) {
-      // the next panel's columns [k, k + 32): their largest magnitude over
-      // the rows below the next block, for its diagonal-block tests (the
-      // 16 threads with the same ty are one half-warp)
-      unsigned long long* nxt =
-          reinterpret_cast<unsigned long long*>(s.dpool + B.xoff + kAppNextColmax);
-#pragma unroll
-      for (int b = 0; b < 2; b++) {
-        double m = 0.0;
-#pragma unroll
-        for (int a = 0; a < 4; a++) {
-          const int i = i0 + tx + 16 * a;
-          if (i < f && i >= k + kBigPanelMax) m = fmax(m, fabs(cur[a][b] - acc[a][b]));
-        }
-#pragma unroll
-        for (int o = 1; o < 16; o <<= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-        const int j = j0 + ty + 16 * b;
-        if (tx == 0 && j < f && m > 0.0)
-          atomicMax(nxt + (ty + 16 * b), (unsigned long long)__double_as_longlong(m));
-      }
-    }
   }
   // close the panel once every CTA is done with the fronts' fields
   __threadfence();
@@ -818,55 +797,26 @@ void assemble_big(const DevPlan& p, const DevState& s, const int* list, int nl, 
   prof.end(kPhBigAsm, stream, 2 + (diag ? 1 : 0) + maxkids);
 }
 
-void update_big(const DevState& s, const int* list, int count, cudaStream_t stream, Prof& prof) {
-  const int upd_grid = 148 * 4;
-  prof.begin(stream);
-  for (int c0 = 0; c0 < count; c0 += kUpdMaxFronts) {
-    const int nl = std::min(kUpdMaxFronts, count - c0);
-    big_update_kernel<<<upd_grid, kUpdThreads, 0, stream>>>(s, list + c0, nl);
-  }
-  prof.end(kPhBigUpd, stream, (count + kUpdMaxFronts - 1) / kUpdMaxFronts);
-}
 
-// Class-6 fronts: blocked panels with a-posteriori tests (big_app.cu). The
-// steps a level needs without failed tests are launched back to back; then
-// the fronts still open (a failed test delays a candidate and shortens its
-// panel) are counted on the device and the loop continues until none is.
+// Class-6 fronts: blocked panels with a-posteriori tests (big_app.cu), all
+// of the level's panel steps in one cooperative launch.
 cudaError_t app_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
                       int maxkids, const FactorParams& prm, const double* vals,
                       const double* diag, cudaStream_t stream, Prof& prof) {
   const int nl = info.count_app;
   const int* list6 = s.class_list + (size_t)6 * p.num_nodes;
   assemble_big(p, s, list6, nl, info.max_f_app, maxkids, vals, diag, stream, prof);
-  int step = 1;
-  int nsteps = (info.max_fs_app + kBigPanelMax - 1) / kBigPanelMax + 1;
-  for (int round = 0;; round++) {
-    for (int t = 0; t < nsteps; t++, step++) {
-      prof.begin(stream);
-      cudaError_t e = launch_app_panel(s, prm, nl, info.max_f_app, list6, step, stream);
-      if (e != cudaSuccess) return e;
-      prof.end(kPhBigPanel, stream, 3);
-      update_big(s, list6, nl, stream, prof);
-      prof.begin(stream);
-      e = launch_app_delay(s, nl, list6, step, stream);
-      if (e != cudaSuccess) return e;
-      prof.end(kPhBigPanel, stream, 1);
-    }
-    cudaError_t e = cudaMemsetAsync(s.big_meta + 19, 0, 2 * sizeof(int), stream);
-    if (e != cudaSuccess) return e;
-    e = launch_app_open_count(s, nl, list6, stream);
-    if (e != cudaSuccess) return e;
-    int open[2] = {0, 0};
-    e = cudaMemcpyAsync(open, s.big_meta + 19, 2 * sizeof(int), cudaMemcpyDeviceToHost, stream);
-    if (e != cudaSuccess) return e;
-    e = cudaStreamSynchronize(stream);
-    if (e != cudaSuccess) return e;
-    if (open[0] == 0) break;
-    // every step accepts a pivot or delays a candidate, so this ends
-    nsteps = (open[1] + kBigPanelMax - 1) / kBigPanelMax + 1;
-    if (round > 4 * (info.max_fs_app + 1)) return cudaErrorUnknown;
-  }
-  return cudaSuccess;
+  prof.begin(stream);
+  cudaError_t e =
+      launch_app_level(s, prm, nl, info.max_fs_app, list6, s.big_meta + 21, stream);
+  if (e != cudaSuccess) return e;
+  prof.end(kPhBigPanel, stream, 1);
+  int cap = 0;
+  e = cudaMemcpyAsync(&cap, s.big_meta + 23, sizeof(int), cudaMemcpyDeviceToHost, stream);
+  if (e != cudaSuccess) return e;
+  e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return e;
+  return cap ? cudaErrorUnknown : cudaSuccess;
 }
 
 }  // namespace

@@ -8,30 +8,30 @@
 // alternative 1x1 at imax or a Duff 2x2, or delays the candidate to the
 // parent. Once the candidates are arranged so that nearly every one passes
 // where it stands (pivot-order reuse), that sequence of column-wide tests is
-// what costs time, not arithmetic. Here a panel of up to 32 candidates is
-// decided in three data-parallel passes instead:
+// what costs time, not arithmetic. Here a panel of up to 32 candidates of
+// every front of a tree level is decided in four data-parallel phases:
 //
-//   1. app_diag_kernel (one CTA per front): the 32 x 32 diagonal block is
-//      factored in shared memory with the reference's tests (one warp decides,
-//      one lane per row; the CTA updates the block). A test's column maximum
-//      joins the block's rows with, for the panel's first pivot, the
-//      column's maximum below the block that the previous panel's trailing
-//      update left behind; a candidate that fails is rotated behind the
-//      block's candidates and delayed. It records, per accepted pivot, the
-//      block part of the column maximum.
-//   2. app_rows_kernel (many CTAs per front): every row below the block forms
-//      its entries of the pivot columns, W = F21 L11^-T (the values the
-//      reference's test sees), stores them for the trailing update, and the
-//      column maxima over all rows below are reduced.
-//   3. app_accept_kernel: the reference's tests are evaluated exactly, with
-//      the column maxima over the whole front; the pivots before the first
+//   D. (one warp per front) Delays left by the previous panel are applied
+//      with the reference's symmetric interchange (symm_swap,
+//      sparse_ldl.h:1270-1292). Then the 32 x 32 diagonal block is factored
+//      in shared memory with the reference's tests (lane r owns block row
+//      r). A test's column maximum joins the block's rows with, for the
+//      panel's first pivot, the column's maximum below the block that the
+//      previous panel's trailing update left behind. A pair that formed a
+//      2x2 pivot in the pivot record is tried as that 2x2 first. A
+//      candidate that fails is rotated behind the block's candidates.
+//   R. (row chunks) Every row below the block forms its entries of the
+//      pivot columns, W = F21 L11^-T (the values the reference's tests see),
+//      stores them for the trailing update, and the column maxima over all
+//      rows below are reduced.
+//   A. (row chunks) The reference's tests are evaluated exactly, with the
+//      column maxima over the whole front; the pivots before the first
 //      failure are accepted and written as L (D on the diagonal, 2x2 blocks
-//      with d21 below it, as the reference stores them). The first failing
-//      pivot, and the candidates that failed in the block before it, are
-//      delayed: after the trailing update
-//      (big_update_kernel) app_delay_kernel moves them behind the remaining
-//      candidates with the reference's symmetric interchange (symm_swap,
-//      sparse_ldl.h:1270-1292), as the reference's delay does.
+//      with d21 below it, as the reference stores them). The first rejected
+//      pivot, and the candidates that failed in the block while only
+//      accepted pivots preceded them, are delayed at the next phase D.
+//   U. (64 x 64 tiles) The trailing matrix gets the rank-kw update of the
+//      accepted pivots.
 //
 // Every accepted pivot therefore satisfies the reference's threshold test
 // against its whole column, so the factorization has the reference's
@@ -39,17 +39,25 @@
 // its inertia; only the order in which candidates are tried differs (a
 // candidate's 2x2 partner is searched within its panel's block).
 //
-// The front stays in HBM in logical order between passes (column-major,
-// lower triangle, the layout big_chain.cu and big_update_kernel use). The
-// panel's state lives in a per-front scratch area (xoff): the block's L,
-// D, tests and permutation. Each pass checks that the scratch belongs to the
-// current step (the step number the diagonal pass stamped), so fronts that
-// finished earlier do nothing and no pass reads the front's descriptor while
-// another pass of the same launch writes it.
+// The phases run in one cooperative launch per level, separated by grid-wide
+// barriers: a panel step costs four barriers instead of five kernel
+// launches. Every CTA runs the same phases and barriers; the loop ends for
+// all of them on a count that the barrier makes visible to all, or at a cap
+// that the progress of every step guarantees not to reach (each step of an
+// active front accepts a pivot or delays a candidate).
+//
+// The front stays in HBM in logical order between steps (column-major,
+// lower triangle, the layout big_chain.cu and big_update_kernel use). A
+// panel's state lives in a per-front scratch area (xoff) stamped with the
+// step number, so a front that finished earlier takes no part.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <climits>
 
 #include "ldl_internal.h"
+
+namespace cg = cooperative_groups;
 
 namespace b200ldl {
 
@@ -57,7 +65,10 @@ namespace {
 
 constexpr int kBlk = 32;  // candidates per panel
 constexpr int kLd = kBlk + 1;
-constexpr int kRowThreads = 256;
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kTileU = 64;          // trailing-update tile
+constexpr int kChunkFronts = 1024;  // fronts per work-item prefix
 
 // per-front scratch (doubles at xoff)
 constexpr int kXNext = kAppNextColmax;      // [32] next panel's column maxima below (bits)
@@ -70,14 +81,14 @@ constexpr int kXInt = kXBelow + kBlk;       // ints from here
 // int offsets (from kXInt as int*)
 constexpr int kIPerm = 0;    // [32] block position -> block position before the panel
 constexpr int kIKind = 32;   // [32] 1: 1x1, 2: first of a 2x2, 3: second of a 2x2
-constexpr int kIDlt = 64;    // [32] candidates delayed in the block: pivots accepted before
+constexpr int kIDlt = 64;    // [32] candidates failed in the block: pivots accepted before
 constexpr int kIAcc = 96;    // pivots accepted inside the block
 constexpr int kINbk = 97;    // candidates in the block
 constexpr int kIK = 98;      // first position of the panel
 constexpr int kIStep = 99;   // step number of the panel
 constexpr int kINcand = 100;
 constexpr int kIMoved = 101;  // 1 if the block permutation is not the identity
-constexpr int kIDcnt = 102;   // candidates to delay after the update
+constexpr int kIDcnt = 102;   // candidates to delay at the next step
 constexpr int kIDpos = 103;   // [32] their positions, decreasing
 constexpr int kINint = kIDpos + kBlk;
 static_assert(kXInt + (kINint + 1) / 2 <= kAppScratch, "a-posteriori scratch size");
@@ -139,303 +150,429 @@ __device__ int passing_prefix(const double* X, double ustab, double tol) {
   return p;
 }
 
-// ---------------------------------------------------------------- pass 1
+// ------------------------------------------------------------- shared memory
 
-constexpr int kDiagThreads = 128;
+struct WarpDiag {  // phase D, one per warp
+  double A[kBlk][kLd];  // the block, symmetric, factored in place
+  double Lb[kBlk][kLd];
+  double dd[3 * kBlk], cin[kBlk], rin[kBlk], below0[kBlk];
+  int perm[kBlk], kind[kBlk], dlt[kBlk];
+};
 
-__global__ void __launch_bounds__(kDiagThreads)
-    app_diag_kernel(DevState s, FactorParams prm, const int* __restrict__ list, int step) {
-  __shared__ double A[kBlk][kLd];   // the block, symmetric, factored in place
-  __shared__ double A0[kBlk][kLd];  // the block before the panel
-  __shared__ double Lb[kBlk][kLd];
-  __shared__ int perm[kBlk], kind[kBlk], dlt[kBlk];
-  __shared__ double dd[3 * kBlk], cin[kBlk], rin[kBlk], below0[kBlk];
-  __shared__ int sh_t, sh_moved;
-  BigFront* B = s.big + list[blockIdx.x];
-  if (B->state != 0) return;  // the same in every thread
+struct RowsSm {  // phases R and A
+  double Ls[kBlk][kLd];
+  double red[kWarps][kBlk];
+  double sd[3 * kBlk], sinv[kBlk];
+  int sperm[kBlk], skind[kBlk];
+  int np;
+};
+
+struct UpdSm {  // phase U
+  double As[kBigPanelMax][kTileU];
+  double Bs[kBigPanelMax][kTileU];
+};
+
+struct Prefix {  // work items of up to kChunkFronts fronts
+  long long ptr[kChunkFronts + 1];
+  long long wsum[kWarps];
+};
+
+constexpr size_t cmax(size_t a, size_t b) { return a > b ? a : b; }
+constexpr size_t kDynSmem = cmax(sizeof(WarpDiag) * kWarps, cmax(sizeof(RowsSm), sizeof(UpdSm)));
+
+// Exclusive prefix of cnt(i) over i in [0, nl) into P.ptr (CTA-wide; nl <=
+// kChunkFronts). Returns the total.
+template <typename Count>
+__device__ long long front_prefix(Prefix& P, int nl, Count cnt) {
+  constexpr int per = kChunkFronts / kThreads;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
-  const int warp = tid >> 5;
+  const int w = tid >> 5;
+  long long c[per];
+  long long mine = 0;
+#pragma unroll
+  for (int u = 0; u < per; u++) {
+    const int i = tid * per + u;
+    c[u] = (i < nl) ? cnt(i) : 0;
+    mine += c[u];
+  }
+  long long incl = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (lane == 31) P.wsum[w] = incl;
+  __syncthreads();
+  long long base = 0;
+  for (int q = 0; q < w; q++) base += P.wsum[q];
+  long long run = base + incl - mine;
+  if (tid == 0) P.ptr[0] = 0;
+#pragma unroll
+  for (int u = 0; u < per; u++) {
+    run += c[u];
+    const int i = tid * per + u;
+    if (i < nl) P.ptr[i + 1] = run;
+  }
+  __syncthreads();
+  return P.ptr[nl];
+}
+
+// front of work item t: the last i with ptr[i] <= t
+__device__ __forceinline__ int item_front(const Prefix& P, int nl, long long t) {
+  int lo = 0, hi = nl;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (P.ptr[mid] <= t)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// ---------------------------------------------------------------- phase D
+
+// Close the previous step of front B (trailing-update work counters, a
+// finished front becomes done), apply the delays it left, and factor the
+// next diagonal block. Returns 1 if the front takes part in this step.
+__device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFront* B, int step,
+                             WarpDiag& w) {
+  const int lane = threadIdx.x & 31;
   const int f = B->f;
-  const int k = B->k;
-  const int ncand = B->ncand;
-  const int nbk = max(0, min(kBlk, ncand - k));
   double* F = s.dpool + B->doff;
   double* Wg = s.dpool + B->woff;
   double* X = s.dpool + B->xoff;
+  int* xi = xint(X);
   int* fv = s.ivars + B->ioff;
   int* orig = fv + f;
-
-  for (int t = tid; t < kBlk * kBlk; t += blockDim.x) {
-    const int i = t % kBlk, j = t / kBlk;
-    const double v = (i < nbk && j < nbk) ? fsym(F, f, k + i, k + j) : 0.0;
-    A[i][j] = v;
-    A0[i][j] = v;
-    Lb[i][j] = 0.0;
+  if (lane == 0 && B->kw > 0) {
+    const double r = (double)(f - B->k);
+    const double fl = r * (r + 1.0) * B->kw;
+    B->flops += fl;
+    atomicAdd(s.flops + 2, fl);
+    atomicAdd(s.flops + 3, 8.0 * (r * (r + 1.0) + 2.0 * r * B->kw));
   }
-  if (tid < kBlk) {
-    perm[tid] = tid;
-    kind[tid] = 0;
-    dlt[tid] = -1;
-    cin[tid] = 0.0;
-    rin[tid] = 0.0;
-    dd[3 * tid] = dd[3 * tid + 1] = dd[3 * tid + 2] = 0.0;
-    // the previous panel's update left these columns' maxima below the block
-    below0[tid] = __longlong_as_double(
-        (long long)reinterpret_cast<unsigned long long*>(X + kXNext)[tid]);
+  __syncwarp();
+  if (lane == 0) {
+    B->kw = 0;
+    if (B->state == 1) B->state = 2;
   }
-  __syncthreads();
-
-  // The reference's tests on the block's candidates in order, one warp, lane
-  // r owning block row r. A test's column maximum joins the block's rows
-  // (exact) with the column's maximum below the block: for the panel's first
-  // pivot that is below0 (exact); after it nothing is known below, so the
-  // maximum used is a lower bound. A candidate that fails a test on a lower
-  // bound fails it on the true maximum as well, so it is delayed for good
-  // (rotated behind the block's candidates, as the reference rotates a
-  // delayed candidate), unless the a-posteriori tests reject a pivot
-  // accepted before it; the accepted ones are checked with the exact maxima
-  // by app_accept_kernel.
-  const double u = prm.ustab, tol = prm.pivot_tol;
-  if (warp == 0) {
-    int t = 0, nr = nbk;
-    while (t < nr) {
-      const double wkk = A[t][t];
-      const bool has = t + 1 < nr;
-      const double at = fabs(A[lane][t]);
-      double bv = (lane > t && lane < nr) ? at : -1.0;
-      int bi = lane;
-      warp_argmax(bv, bi);
-      const double abswik = has ? bv : 0.0;
-      const int imax = has ? bi : t;
-      // block rows that are not candidates any more (rotated behind)
-      const double cnc = warp_max((lane >= nr && lane < nbk) ? at : 0.0);
-      const double col_in = fmax(abswik, cnc);
-      const double colmax = fmax(col_in, t == 0 ? below0[perm[t]] : 0.0);
-      int stp = 0, kpiv = t;
-      double row_in = 0.0;
-      // a pair that formed a 2x2 pivot in the pivot record is tried as that
-      // 2x2 first (the Duff test, as below), since a 1x1 test that sees only
-      // the block's rows would accept the first of them alone and the
-      // a-posteriori test would then reject it
-      bool hinted = false;
-      if (has && s.partner) {
-        const int vt = fv[k + perm[t]], vn = fv[k + perm[t + 1]];
-        hinted = vt >= 0 && vn >= 0 && s.partner[vt] == vn;
-      }
-      if (hinted) {
-        const double r2 =
-            warp_max((lane >= t && lane < nbk && lane != t + 1) ? fabs(A[lane][t + 1]) : 0.0);
-        const double rm2 = fmax(r2, t == 0 ? below0[perm[t + 1]] : 0.0);
-        const double w21 = A[t + 1][t], w22 = A[t + 1][t + 1];
-        const double det = fabs(wkk * w22 - w21 * w21);
-        if (det >= tol) {
-          const double delta = det / fmax(fabs(w22) + fabs(w21), fabs(wkk) + fabs(w21));
-          if (delta >= u * colmax && delta >= u * rm2) {
-            stp = 2;
-            kpiv = t + 1;
-            row_in = r2;
+  __syncwarp();
+  if (B->pending > 0 && B->state == 0) {
+    // the candidates to delay move behind the remaining candidates, largest
+    // position first so that no interchange moves another one still to go
+    const int nd = xi[kIDcnt];
+    const int k = B->k;
+    int ncand = B->ncand;
+    for (int q = 0; q < nd; q++) {
+      const int a = xi[kIDpos + q];
+      const int b = ncand - 1;
+      if (a < b) {
+        for (int j = lane; j < f; j += 32) {
+          double *p, *r;
+          if (j < a) {
+            p = F + a + (size_t)f * j;
+            r = F + b + (size_t)f * j;
+          } else if (j == a) {
+            p = F + a + (size_t)f * a;
+            r = F + b + (size_t)f * b;
+          } else if (j < b) {
+            p = F + j + (size_t)f * a;
+            r = F + b + (size_t)f * j;
+          } else if (j == b) {
+            continue;
+          } else {
+            p = F + j + (size_t)f * a;
+            r = F + j + (size_t)f * b;
           }
-        }
-      }
-      if (stp != 0) {
-        // taken as recorded
-      } else if (fabs(wkk) >= tol && fabs(wkk) >= u * colmax) {
-        stp = 1;
-      } else if (has) {
-        row_in = warp_max((lane >= t && lane < nbk && lane != imax) ? fabs(A[lane][imax]) : 0.0);
-        const double rowmax = fmax(row_in, t == 0 ? below0[perm[imax]] : 0.0);
-        const double wii = A[imax][imax], wik = A[imax][t];
-        if (fabs(wii) >= tol && fabs(wii) >= u * rowmax) {
-          stp = 1;
-          kpiv = imax;
-        } else {
-          const double det = fabs(wkk * wii - wik * wik);
-          if (det >= tol) {
-            const double delta = det / fmax(fabs(wii) + abswik, fabs(wkk) + abswik);
-            if (delta >= u * colmax && delta >= u * rowmax) {
-              stp = 2;
-              kpiv = imax;
-            }
-          }
-        }
-      }
-      // interchange: the accepted pivot to position t (+1), or the failing
-      // candidate behind the block's candidates
-      const int ksrc = (stp == 0) ? t : t + stp - 1;
-      const int kdst = (stp == 0) ? nr - 1 : kpiv;
-      if (ksrc != kdst) {
-        {
-          const double x = A[ksrc][lane];
-          A[ksrc][lane] = A[kdst][lane];
-          A[kdst][lane] = x;
-          const double y = Lb[ksrc][lane];
-          Lb[ksrc][lane] = Lb[kdst][lane];
-          Lb[kdst][lane] = y;
-        }
-        __syncwarp();
-        {
-          const double x = A[lane][ksrc];
-          A[lane][ksrc] = A[lane][kdst];
-          A[lane][kdst] = x;
+          const double t = *p;
+          *p = *r;
+          *r = t;
         }
         if (lane == 0) {
-          int q = perm[ksrc];
-          perm[ksrc] = perm[kdst];
-          perm[kdst] = q;
-          q = dlt[ksrc];
-          dlt[ksrc] = dlt[kdst];
-          dlt[kdst] = q;
-        }
-        __syncwarp();
-      }
-      if (stp == 0) {
-        if (lane == 0) dlt[nr - 1] = t;
-        __syncwarp();
-        nr--;
-        continue;
-      }
-      if (stp == 1) {
-        const double d = A[t][t];
-        const double li = A[lane][t] * (1.0 / d);
-        if (lane > t && lane < nbk) Lb[lane][t] = li;
-        if (lane == 0) {
-          kind[t] = 1;
-          dd[3 * t] = d;
-          cin[t] = (kpiv == t) ? col_in : row_in;
-        }
-      } else {
-        const double d11 = A[t][t], d21 = A[t + 1][t], d22 = A[t + 1][t + 1];
-        const double di = 1.0 / (d11 * d22 - d21 * d21);
-        const double i00 = d22 * di, i01 = -d21 * di, i11 = d11 * di;
-        const double a = A[lane][t], b = A[lane][t + 1];
-        if (lane > t + 1 && lane < nbk) {
-          Lb[lane][t] = a * i00 + b * i01;
-          Lb[lane][t + 1] = a * i01 + b * i11;
-        }
-        if (lane == 0) {
-          kind[t] = 2;
-          kind[t + 1] = 3;
-          dd[3 * t] = d11;
-          dd[3 * t + 1] = d21;
-          dd[3 * t + 2] = d22;
-          cin[t] = col_in;
-          rin[t] = row_in;
+          int t = fv[a];
+          fv[a] = fv[b];
+          fv[b] = t;
+          t = orig[a];
+          orig[a] = orig[b];
+          orig[b] = t;
+          // columns that moved lose their estimate
+          if (a - k < kBlk) X[kXNext + (a - k)] = 0.0;
+          if (b - k < kBlk) X[kXNext + (b - k)] = 0.0;
         }
       }
+      ncand--;
       __syncwarp();
-      // rank-1 or rank-2 update of the block's remaining rows and columns
-      // (rotated ones included): entry (i, j) gets L(max) W(min) in both
-      // triangles, the lower-triangle product of the reference's update. The
-      // column loop is unrolled so that its loads are in flight together.
-      const int t1 = t + stp;
-      if (lane >= t1 && lane < nbk) {
-#pragma unroll
-        for (int c = 0; c < kBlk; c++) {
-          if (c >= t1 && c < nbk) {
-            const int hi = max(lane, c), lo = min(lane, c);
-            double v = A[lane][c] - Lb[hi][t] * A[lo][t];
-            if (stp == 2) v -= Lb[hi][t + 1] * A[lo][t + 1];
-            A[lane][c] = v;
-          }
-        }
-      }
-      __syncwarp();
-      t = t1;
     }
-    if (lane == 0) sh_t = t;
+    if (lane == 0) {
+      B->ncand = ncand;
+      B->pending = 0;
+      if (B->k >= ncand) B->state = 2;
+    }
+    __syncwarp();
   }
-  __syncthreads();
-  const int acc = sh_t;
-  if (warp == 0) {
-    const bool moved = (lane < nbk) && perm[lane] != lane;
-    const unsigned mv = __ballot_sync(0xffffffffu, moved);
-    if (lane == 0) sh_moved = mv != 0u;
-  }
-  __syncthreads();
-  const int moved = sh_moved;
+  if (B->state != 0) return 0;
 
-  // panel state for the next passes
-  for (int t = tid; t < kBlk * kLd; t += blockDim.x) X[kXL + t] = (&Lb[0][0])[t];
-  if (tid < kBlk) {
-    X[kXD + 3 * tid] = dd[3 * tid];
-    X[kXD + 3 * tid + 1] = dd[3 * tid + 1];
-    X[kXD + 3 * tid + 2] = dd[3 * tid + 2];
-    X[kXCin + tid] = cin[tid];
-    X[kXRin + tid] = rin[tid];
-    X[kXBelow + tid] = 0.0;
-    int* xi = xint(X);
-    xi[kIPerm + tid] = perm[tid];
-    xi[kIKind + tid] = kind[tid];
-    xi[kIDlt + tid] = dlt[tid];
+  const int k = B->k;
+  const int ncand = B->ncand;
+  const int nbk = max(0, min(kBlk, ncand - k));
+  for (int t = lane; t < kBlk * kBlk; t += 32) {
+    const int i = t % kBlk, j = t / kBlk;
+    w.A[i][j] = (i < nbk && j < nbk) ? fsym(F, f, k + i, k + j) : 0.0;
+    w.Lb[i][j] = 0.0;
   }
-  if (tid == 0) {
-    int* xi = xint(X);
+  w.perm[lane] = lane;
+  w.kind[lane] = 0;
+  w.dlt[lane] = -1;
+  w.cin[lane] = 0.0;
+  w.rin[lane] = 0.0;
+  w.dd[3 * lane] = w.dd[3 * lane + 1] = w.dd[3 * lane + 2] = 0.0;
+  w.below0[lane] = __longlong_as_double(
+      (long long)reinterpret_cast<unsigned long long*>(X + kXNext)[lane]);
+  __syncwarp();
+
+  // The reference's tests on the block's candidates in order. For the
+  // panel's first pivot the column maximum below the block is exact
+  // (below0); after it nothing is known below, so the maximum used is a
+  // lower bound: a candidate that fails on a lower bound fails on the true
+  // maximum as well, so it is delayed, unless the a-posteriori tests reject
+  // a pivot accepted before it. Accepted pivots are checked with the exact
+  // maxima in phase A.
+  const double u = prm.ustab, tol = prm.pivot_tol;
+  int t = 0, nr = nbk;
+  while (t < nr) {
+    const double wkk = w.A[t][t];
+    const bool has = t + 1 < nr;
+    const double at = fabs(w.A[lane][t]);
+    double bv = (lane > t && lane < nr) ? at : -1.0;
+    int bi = lane;
+    warp_argmax(bv, bi);
+    const double abswik = has ? bv : 0.0;
+    const int imax = has ? bi : t;
+    // block rows that are not candidates any more (rotated behind)
+    const double cnc = (nr < nbk) ? warp_max((lane >= nr && lane < nbk) ? at : 0.0) : 0.0;
+    const double col_in = fmax(abswik, cnc);
+    const double colmax = fmax(col_in, t == 0 ? w.below0[w.perm[t]] : 0.0);
+    int stp = 0, kpiv = t;
+    double row_in = 0.0;
+    // a pair that formed a 2x2 pivot in the pivot record is tried as that
+    // 2x2 first (the Duff test), since a 1x1 test that sees only the block's
+    // rows would accept the first of them alone and the a-posteriori test
+    // would then reject it
+    bool hinted = false;
+    if (has && s.partner) {
+      const int vt = fv[k + w.perm[t]], vn = fv[k + w.perm[t + 1]];
+      hinted = vt >= 0 && vn >= 0 && s.partner[vt] == vn;
+    }
+    if (hinted) {
+      const double r2 =
+          warp_max((lane >= t && lane < nbk && lane != t + 1) ? fabs(w.A[lane][t + 1]) : 0.0);
+      const double rm2 = fmax(r2, t == 0 ? w.below0[w.perm[t + 1]] : 0.0);
+      const double w21 = w.A[t + 1][t], w22 = w.A[t + 1][t + 1];
+      const double det = fabs(wkk * w22 - w21 * w21);
+      if (det >= tol) {
+        const double delta = det / fmax(fabs(w22) + fabs(w21), fabs(wkk) + fabs(w21));
+        if (delta >= u * colmax && delta >= u * rm2) {
+          stp = 2;
+          kpiv = t + 1;
+          row_in = r2;
+        }
+      }
+    }
+    if (stp != 0) {
+      // taken as recorded
+    } else if (fabs(wkk) >= tol && fabs(wkk) >= u * colmax) {
+      stp = 1;
+    } else if (has) {
+      row_in = warp_max((lane >= t && lane < nbk && lane != imax) ? fabs(w.A[lane][imax]) : 0.0);
+      const double rowmax = fmax(row_in, t == 0 ? w.below0[w.perm[imax]] : 0.0);
+      const double wii = w.A[imax][imax], wik = w.A[imax][t];
+      if (fabs(wii) >= tol && fabs(wii) >= u * rowmax) {
+        stp = 1;
+        kpiv = imax;
+      } else {
+        const double det = fabs(wkk * wii - wik * wik);
+        if (det >= tol) {
+          const double delta = det / fmax(fabs(wii) + abswik, fabs(wkk) + abswik);
+          if (delta >= u * colmax && delta >= u * rowmax) {
+            stp = 2;
+            kpiv = imax;
+          }
+        }
+      }
+    }
+    // interchange: the accepted pivot to position t (+1), or the failing
+    // candidate behind the block's candidates
+    const int ksrc = (stp == 0) ? t : t + stp - 1;
+    const int kdst = (stp == 0) ? nr - 1 : kpiv;
+    if (ksrc != kdst) {
+      {
+        const double x = w.A[ksrc][lane];
+        w.A[ksrc][lane] = w.A[kdst][lane];
+        w.A[kdst][lane] = x;
+        const double y = w.Lb[ksrc][lane];
+        w.Lb[ksrc][lane] = w.Lb[kdst][lane];
+        w.Lb[kdst][lane] = y;
+      }
+      __syncwarp();
+      {
+        const double x = w.A[lane][ksrc];
+        w.A[lane][ksrc] = w.A[lane][kdst];
+        w.A[lane][kdst] = x;
+      }
+      if (lane == 0) {
+        int q = w.perm[ksrc];
+        w.perm[ksrc] = w.perm[kdst];
+        w.perm[kdst] = q;
+        q = w.dlt[ksrc];
+        w.dlt[ksrc] = w.dlt[kdst];
+        w.dlt[kdst] = q;
+      }
+      __syncwarp();
+    }
+    if (stp == 0) {
+      if (lane == 0) w.dlt[nr - 1] = t;
+      __syncwarp();
+      nr--;
+      continue;
+    }
+    if (stp == 1) {
+      const double d = w.A[t][t];
+      const double li = w.A[lane][t] * (1.0 / d);
+      if (lane > t && lane < nbk) w.Lb[lane][t] = li;
+      if (lane == 0) {
+        w.kind[t] = 1;
+        w.dd[3 * t] = d;
+        w.cin[t] = (kpiv == t) ? col_in : row_in;
+      }
+    } else {
+      const double d11 = w.A[t][t], d21 = w.A[t + 1][t], d22 = w.A[t + 1][t + 1];
+      const double di = 1.0 / (d11 * d22 - d21 * d21);
+      const double i00 = d22 * di, i01 = -d21 * di, i11 = d11 * di;
+      const double a = w.A[lane][t], b = w.A[lane][t + 1];
+      if (lane > t + 1 && lane < nbk) {
+        w.Lb[lane][t] = a * i00 + b * i01;
+        w.Lb[lane][t + 1] = a * i01 + b * i11;
+      }
+      if (lane == 0) {
+        w.kind[t] = 2;
+        w.kind[t + 1] = 3;
+        w.dd[3 * t] = d11;
+        w.dd[3 * t + 1] = d21;
+        w.dd[3 * t + 2] = d22;
+        w.cin[t] = col_in;
+        w.rin[t] = row_in;
+      }
+    }
+    __syncwarp();
+    // rank-1 or rank-2 update of the block's remaining rows and columns
+    // (rotated ones included): entry (i, j) gets L(max) W(min) in both
+    // triangles, the lower-triangle product of the reference's update. The
+    // column loop is unrolled so that its loads are in flight together.
+    const int t1 = t + stp;
+    if (lane >= t1 && lane < nbk) {
+#pragma unroll
+      for (int c = 0; c < kBlk; c++) {
+        if (c >= t1 && c < nbk) {
+          const int hi = max(lane, c), lo = min(lane, c);
+          double v = w.A[lane][c] - w.Lb[hi][t] * w.A[lo][t];
+          if (stp == 2) v -= w.Lb[hi][t + 1] * w.A[lo][t + 1];
+          w.A[lane][c] = v;
+        }
+      }
+    }
+    __syncwarp();
+    t = t1;
+  }
+  const int acc = t;
+  const bool moved = __ballot_sync(0xffffffffu, lane < nbk && w.perm[lane] != lane) != 0u;
+
+  // panel state for phases R and A
+  for (int q = lane; q < kBlk * kLd; q += 32) X[kXL + q] = (&w.Lb[0][0])[q];
+  X[kXD + 3 * lane] = w.dd[3 * lane];
+  X[kXD + 3 * lane + 1] = w.dd[3 * lane + 1];
+  X[kXD + 3 * lane + 2] = w.dd[3 * lane + 2];
+  X[kXCin + lane] = w.cin[lane];
+  X[kXRin + lane] = w.rin[lane];
+  X[kXBelow + lane] = 0.0;
+  xi[kIPerm + lane] = w.perm[lane];
+  xi[kIKind + lane] = w.kind[lane];
+  xi[kIDlt + lane] = w.dlt[lane];
+  if (lane == 0) {
     xi[kIAcc] = acc;
     xi[kINbk] = nbk;
     xi[kIK] = k;
     xi[kIStep] = step;
     xi[kINcand] = ncand;
-    xi[kIMoved] = moved;
+    xi[kIMoved] = moved ? 1 : 0;
   }
   // the W values of the block rows for the trailing update
-  for (int t = tid; t < kBlk * kBlk; t += blockDim.x) {
-    const int i = t % kBlk, p = t / kBlk;
-    if (p < acc && i > p && i < nbk) Wg[(size_t)p * f + k + i] = A[i][p];
+  for (int q = lane; q < kBlk * kBlk; q += 32) {
+    const int i = q % kBlk, p = q / kBlk;
+    if (p < acc && i > p && i < nbk) Wg[(size_t)p * f + k + i] = w.A[i][p];
   }
   if (moved) {
-    // the block's rows and columns follow the interchanges: the block itself
-    // and the variables here; the factor rows of earlier panels in
-    // app_rows_kernel
-    for (int t = tid; t < kBlk * kBlk; t += blockDim.x) {
-      const int i = t % kBlk, j = t / kBlk;
-      if (j <= i && i < nbk) F[(k + i) + (size_t)f * (k + j)] = A0[perm[i]][perm[j]];
-    }
-    int a = 0, b = 0;
-    if (tid < nbk) {
-      a = fv[k + perm[tid]];
-      b = orig[k + perm[tid]];
-    }
-    __syncthreads();
-    if (tid < nbk) {
-      fv[k + tid] = a;
-      orig[k + tid] = b;
+    // the block itself and the variables follow the interchanges (the factor
+    // rows of earlier panels move in phase R): lane i gathers its row
+    // before any lane writes
+    double v[kBlk];
+#pragma unroll
+    for (int j = 0; j < kBlk; j++)
+      v[j] = (j <= lane && lane < nbk) ? fsym(F, f, k + w.perm[lane], k + w.perm[j]) : 0.0;
+    const int a = (lane < nbk) ? fv[k + w.perm[lane]] : 0;
+    const int b = (lane < nbk) ? orig[k + w.perm[lane]] : 0;
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < kBlk; j++)
+      if (j <= lane && lane < nbk) F[(k + lane) + (size_t)f * (k + j)] = v[j];
+    if (lane < nbk) {
+      fv[k + lane] = a;
+      orig[k + lane] = b;
     }
   }
+  __syncwarp();
+  return 1;
 }
 
-// ---------------------------------------------------------------- pass 2
+// ---------------------------------------------------------------- phase R
 
-__global__ void __launch_bounds__(kRowThreads)
-    app_rows_kernel(DevState s, const int* __restrict__ list, int step) {
-  __shared__ double Ls[kBlk][kLd];
-  __shared__ int sperm[kBlk];
-  __shared__ double red[kRowThreads / 32][kBlk];
-  const BigFront* B = s.big + list[blockIdx.x];
-  double* X = s.dpool + B->xoff;
-  const int* xi = xint(X);
-  if (xi[kIStep] != step) return;  // the same in every thread
+__device__ __forceinline__ bool active(const DevState& s, const BigFront& B, int step) {
+  return xint(s.dpool + B.xoff)[kIStep] == step;
+}
+
+// row chunks of an active front in phases R and A (at least one, which also
+// carries the moves of earlier factor rows)
+__device__ __forceinline__ int row_chunks(const DevState& s, const BigFront& B, int step) {
+  if (!active(s, B, step)) return 0;
+  const int* xi = xint(s.dpool + B.xoff);
+  const int rows = B.f - (xi[kIK] + xi[kINbk]);
+  return max(1, (rows + kThreads - 1) / kThreads);
+}
+
+__device__ void phase_r_item(const DevState& s, const BigFront& B, int chunk, int nchunk,
+                             RowsSm& sm) {
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
-  const int f = B->f;
+  double* X = s.dpool + B.xoff;
+  const int* xi = xint(X);
+  const int f = B.f;
   const int k = xi[kIK];
   const int nbk = xi[kINbk];
   const int acc = xi[kIAcc];
   const int moved = xi[kIMoved];
-  for (int t = tid; t < kBlk * kLd; t += blockDim.x) (&Ls[0][0])[t] = X[kXL + t];
-  if (tid < kBlk) sperm[tid] = xi[kIPerm + tid];
+  for (int t = tid; t < kBlk * kLd; t += kThreads) (&sm.Ls[0][0])[t] = X[kXL + t];
+  if (tid < kBlk) sm.sperm[tid] = xi[kIPerm + tid];
   __syncthreads();
-  double* F = s.dpool + B->doff;
-  double* Wg = s.dpool + B->woff;
+  double* F = s.dpool + B.doff;
+  double* Wg = s.dpool + B.woff;
   if (moved) {
     // the block's rows in the factor columns of earlier panels: one warp per
     // column, lane i moves row k + perm[i] to row k + i
-    const int gw = blockIdx.y * (kRowThreads / 32) + warp;
-    const int nw = gridDim.y * (kRowThreads / 32);
-    const bool mv = lane < nbk && sperm[lane] != lane;
-    for (int j = gw; j < k; j += nw) {
-      const double v = mv ? F[(k + sperm[lane]) + (size_t)f * j] : 0.0;
+    const bool mv = lane < nbk && sm.sperm[lane] != lane;
+    for (int j = chunk * kWarps + warp; j < k; j += nchunk * kWarps) {
+      const double v = mv ? F[(k + sm.sperm[lane]) + (size_t)f * j] : 0.0;
       __syncwarp();
       if (mv) F[(k + lane) + (size_t)f * j] = v;
     }
@@ -443,11 +580,11 @@ __global__ void __launch_bounds__(kRowThreads)
   double cm[kBlk];
 #pragma unroll
   for (int p = 0; p < kBlk; p++) cm[p] = 0.0;
-  const int r0 = k + nbk;
-  for (int r = r0 + blockIdx.y * kRowThreads + tid; r < f; r += gridDim.y * kRowThreads) {
+  const int r = k + nbk + chunk * kThreads + tid;
+  if (r < f) {
     double a[kBlk];
 #pragma unroll
-    for (int j = 0; j < kBlk; j++) a[j] = (j < nbk) ? F[r + (size_t)f * (k + sperm[j])] : 0.0;
+    for (int j = 0; j < kBlk; j++) a[j] = (j < nbk) ? F[r + (size_t)f * (k + sm.sperm[j])] : 0.0;
     if (moved) {
 #pragma unroll
       for (int j = 0; j < kBlk; j++)
@@ -457,12 +594,12 @@ __global__ void __launch_bounds__(kRowThreads)
 #pragma unroll
     for (int p = 0; p < kBlk; p++) {
       if (p < acc) {
-        double w = a[p];
+        double wv = a[p];
 #pragma unroll
-        for (int q = 0; q < p; q++) w = fma(-a[q], Ls[p][q], w);
-        a[p] = w;
-        Wg[(size_t)p * f + r] = w;
-        cm[p] = fmax(cm[p], fabs(w));
+        for (int q = 0; q < p; q++) wv = fma(-a[q], sm.Ls[p][q], wv);
+        a[p] = wv;
+        Wg[(size_t)p * f + r] = wv;
+        cm[p] = fabs(wv);
       }
     }
   }
@@ -471,55 +608,52 @@ __global__ void __launch_bounds__(kRowThreads)
 #pragma unroll
   for (int p = 0; p < kBlk; p++) {
     const double v = warp_max(cm[p]);
-    if (lane == 0) red[warp][p] = v;
+    if (lane == 0) sm.red[warp][p] = v;
   }
   __syncthreads();
-  if (tid < kBlk && tid < acc) {
+  if (tid < acc) {
     double v = 0.0;
-    for (int w = 0; w < kRowThreads / 32; w++) v = fmax(v, red[w][tid]);
-    atomicMax(reinterpret_cast<unsigned long long*>(X + kXBelow) + tid,
-              (unsigned long long)__double_as_longlong(v));
+    for (int q = 0; q < kWarps; q++) v = fmax(v, sm.red[q][tid]);
+    if (v > 0.0)
+      atomicMax(reinterpret_cast<unsigned long long*>(X + kXBelow) + tid,
+                (unsigned long long)__double_as_longlong(v));
   }
+  __syncthreads();
 }
 
-// ---------------------------------------------------------------- pass 3
+// ---------------------------------------------------------------- phase A
 
-__global__ void __launch_bounds__(kRowThreads)
-    app_accept_kernel(DevState s, FactorParams prm, const int* __restrict__ list, int step) {
-  __shared__ double Ls[kBlk][kLd];
-  __shared__ double sd[3 * kBlk], sinv[kBlk];
-  __shared__ int skind[kBlk];
-  __shared__ int sh_np;
-  BigFront* B = s.big + list[blockIdx.x];
+__device__ void phase_a_item(const DevState& s, const FactorParams& prm, BigFront* B, int chunk,
+                             RowsSm& sm) {
+  const int tid = threadIdx.x;
   double* X = s.dpool + B->xoff;
   int* xi = xint(X);
-  if (xi[kIStep] != step) return;  // the same in every thread
-  const int tid = threadIdx.x;
   const int f = B->f;
   const int k = xi[kIK];
   const int nbk = xi[kINbk];
-  if (tid == 0) sh_np = passing_prefix(X, prm.ustab, prm.pivot_tol);
-  for (int t = tid; t < kBlk * kLd; t += blockDim.x) (&Ls[0][0])[t] = X[kXL + t];
+  if (tid == 0) sm.np = passing_prefix(X, prm.ustab, prm.pivot_tol);
+  for (int t = tid; t < kBlk * kLd; t += kThreads) (&sm.Ls[0][0])[t] = X[kXL + t];
   if (tid < kBlk) {
-    skind[tid] = xi[kIKind + tid];
-    sd[3 * tid] = X[kXD + 3 * tid];
-    sd[3 * tid + 1] = X[kXD + 3 * tid + 1];
-    sd[3 * tid + 2] = X[kXD + 3 * tid + 2];
+    sm.skind[tid] = xi[kIKind + tid];
+    sm.sd[3 * tid] = X[kXD + 3 * tid];
+    sm.sd[3 * tid + 1] = X[kXD + 3 * tid + 1];
+    sm.sd[3 * tid + 2] = X[kXD + 3 * tid + 2];
     // 1x1 pivots scale their column by 1/d, as the reference does
-    sinv[tid] = (xi[kIKind + tid] == 1) ? 1.0 / X[kXD + 3 * tid] : 0.0;
+    sm.sinv[tid] = (xi[kIKind + tid] == 1) ? 1.0 / X[kXD + 3 * tid] : 0.0;
   }
   __syncthreads();
-  const int np = sh_np;
+  const int np = sm.np;
   double* F = s.dpool + B->doff;
   const double* Wg = s.dpool + B->woff;
   // L of the accepted pivots on the rows below the block
-  for (int r = k + nbk + blockIdx.y * kRowThreads + tid; r < f; r += gridDim.y * kRowThreads) {
+  const int r = k + nbk + chunk * kThreads + tid;
+  if (r < f) {
     for (int p = 0; p < np;) {
-      if (skind[p] == 1) {
-        F[r + (size_t)f * (k + p)] = Wg[(size_t)p * f + r] * sinv[p];
+      if (sm.skind[p] == 1) {
+        F[r + (size_t)f * (k + p)] = Wg[(size_t)p * f + r] * sm.sinv[p];
         p += 1;
       } else {
-        const double d11 = sd[3 * p], d21 = sd[3 * p + 1], d22 = sd[3 * p + 2];
+        const double d11 = sm.sd[3 * p], d21 = sm.sd[3 * p + 1], d22 = sm.sd[3 * p + 2];
         const double di = 1.0 / (d11 * d22 - d21 * d21);
         const double a = Wg[(size_t)p * f + r], b = Wg[(size_t)(p + 1) * f + r];
         F[r + (size_t)f * (k + p)] = a * (d22 * di) + b * (-d21 * di);
@@ -528,182 +662,299 @@ __global__ void __launch_bounds__(kRowThreads)
       }
     }
   }
-  if (blockIdx.y != 0) return;
-  // the block's rows: D on the diagonal (d21 below a 2x2's first column), L
-  for (int t = tid; t < kBlk * kBlk; t += blockDim.x) {
-    const int i = t % kBlk, p = t / kBlk;
-    if (p >= np || i < p || i >= nbk) continue;
-    double v;
-    if (i == p)
-      v = (skind[p] == 3) ? sd[3 * (p - 1) + 2] : sd[3 * p];
-    else if (i == p + 1 && skind[p] == 2)
-      v = sd[3 * p + 1];
-    else
-      v = Ls[i][p];
-    F[(k + i) + (size_t)f * (k + p)] = v;
-  }
-  if (tid != 0) return;
-  // commit the panel (no other CTA reads the descriptor in this pass)
-  int* fv = s.ivars + B->ioff;
-  int npos = 0, nneg = 0;
-  double flops = 0.0;
-  for (int p = 0; p < np;) {
-    if (skind[p] == 1) {
-      if (sd[3 * p] >= 0.0)
-        npos++;
+  if (chunk == 0) {
+    // the block's rows: D on the diagonal (d21 below a 2x2's first column), L
+    for (int t = tid; t < kBlk * kBlk; t += kThreads) {
+      const int i = t % kBlk, p = t / kBlk;
+      if (p >= np || i < p || i >= nbk) continue;
+      double v;
+      if (i == p)
+        v = (sm.skind[p] == 3) ? sm.sd[3 * (p - 1) + 2] : sm.sd[3 * p];
+      else if (i == p + 1 && sm.skind[p] == 2)
+        v = sm.sd[3 * p + 1];
       else
-        nneg++;
-      flops += 2.0 * (double)(f - k - p) * (p + 1);
-      p += 1;
-    } else {
-      const double d11 = sd[3 * p], d21 = sd[3 * p + 1], d22 = sd[3 * p + 2];
-      const double det = d11 * d22 - d21 * d21;
-      if (det >= 0.0) {
-        if (d11 >= 0.0)
-          npos += 2;
-        else
-          nneg += 2;
-      } else {
-        npos++;
-        nneg++;
-      }
-      fv[k + p] = -(fv[k + p] + 1);
-      fv[k + p + 1] = -(fv[k + p + 1] + 1);
-      flops += 4.0 * (double)(f - k - p) * (p + 2);
-      p += 2;
+        v = sm.Ls[i][p];
+      F[(k + i) + (size_t)f * (k + p)] = v;
     }
-  }
-  // candidates to delay: those that failed in the block while only pivots
-  // that are now accepted preceded them, and the first pivot the
-  // a-posteriori tests reject (positions decreasing); candidates that failed
-  // after a rejected pivot are tried again
-  const int acc = xi[kIAcc];
-  const int ncand = xi[kINcand];
-  int nd = 0;
-  for (int q = nbk - 1; q >= acc; q--)
-    if (xi[kIDlt + q] >= 0 && xi[kIDlt + q] <= np) xi[kIDpos + nd++] = k + q;
-  if (np < acc) xi[kIDpos + nd++] = k + np;
-  xi[kIDcnt] = nd;
-  B->kstart = k;
-  B->kw = np;
-  B->k = k + np;
-  B->pending = nd;
-  B->npos += npos;
-  B->nneg += nneg;
-  B->flops += flops;
-  atomicAdd(s.flops + 1, flops);
-  atomicAdd(s.flops + 5, 1.0);
-  if (np < acc) atomicAdd(s.flops + 6, 1.0);
-  atomicAdd(s.flops + 7, (double)(nd - (np < acc ? 1 : 0)));
-  // the next panel's column maxima, filled by the trailing update
-  for (int j = 0; j < kBlk; j++) X[kXNext + j] = 0.0;
-  B->state = (nd == 0 && k + np >= ncand) ? 1 : 0;
-}
-
-// ---------------------------------------------------------------- delay
-
-// After the trailing update: each candidate to delay moves behind the
-// remaining candidates (the reference's symm_swap with ncand - 1), largest
-// position first so that no interchange moves another one still to go.
-__global__ void app_delay_kernel(DevState s, const int* __restrict__ list, int step) {
-  BigFront* B = s.big + list[blockIdx.x];
-  double* X = s.dpool + B->xoff;
-  const int* xi = xint(X);
-  if (xi[kIStep] != step) return;  // the same in every thread
-  const int nd = xi[kIDcnt];
-  if (nd <= 0) return;
-  const int f = B->f;
-  const int k = B->k;
-  int ncand = B->ncand;
-  double* F = s.dpool + B->doff;
-  int* fv = s.ivars + B->ioff;
-  int* orig = fv + f;
-  double* next = X + kXNext;
-  for (int q = 0; q < nd; q++) {
-    const int a = xi[kIDpos + q];
-    const int b = ncand - 1;
-    if (a < b) {
-      for (int j = threadIdx.x; j < f; j += blockDim.x) {
-        double *p, *r;
-        if (j < a) {
-          p = F + a + (size_t)f * j;
-          r = F + b + (size_t)f * j;
-        } else if (j == a) {
-          p = F + a + (size_t)f * a;
-          r = F + b + (size_t)f * b;
-        } else if (j < b) {
-          p = F + j + (size_t)f * a;
-          r = F + b + (size_t)f * j;
-        } else if (j == b) {
-          continue;
+    if (tid == 0) {
+      // commit the panel (the other items of this front read only the
+      // scratch, never the descriptor)
+      int* fv = s.ivars + B->ioff;
+      int npos = 0, nneg = 0;
+      double flops = 0.0;
+      for (int p = 0; p < np;) {
+        if (sm.skind[p] == 1) {
+          if (sm.sd[3 * p] >= 0.0)
+            npos++;
+          else
+            nneg++;
+          flops += 2.0 * (double)(f - k - p) * (p + 1);
+          p += 1;
         } else {
-          p = F + j + (size_t)f * a;
-          r = F + j + (size_t)f * b;
+          const double d11 = sm.sd[3 * p], d21 = sm.sd[3 * p + 1], d22 = sm.sd[3 * p + 2];
+          const double det = d11 * d22 - d21 * d21;
+          if (det >= 0.0) {
+            if (d11 >= 0.0)
+              npos += 2;
+            else
+              nneg += 2;
+          } else {
+            npos++;
+            nneg++;
+          }
+          fv[k + p] = -(fv[k + p] + 1);
+          fv[k + p + 1] = -(fv[k + p + 1] + 1);
+          flops += 4.0 * (double)(f - k - p) * (p + 2);
+          p += 2;
         }
-        const double t = *p;
-        *p = *r;
-        *r = t;
       }
-      if (threadIdx.x == 0) {
-        int t = fv[a];
-        fv[a] = fv[b];
-        fv[b] = t;
-        t = orig[a];
-        orig[a] = orig[b];
-        orig[b] = t;
-        // columns that moved lose their estimate
-        if (a - k < kBlk) next[a - k] = 0.0;
-        if (b - k < kBlk) next[b - k] = 0.0;
-      }
+      // candidates to delay: those that failed in the block while only
+      // pivots that are now accepted preceded them, and the first pivot the
+      // a-posteriori tests reject (positions decreasing); candidates that
+      // failed after a rejected pivot are tried again
+      const int acc = xi[kIAcc];
+      const int ncand = xi[kINcand];
+      int nd = 0;
+      for (int q = nbk - 1; q >= acc; q--)
+        if (xi[kIDlt + q] >= 0 && xi[kIDlt + q] <= np) xi[kIDpos + nd++] = k + q;
+      if (np < acc) xi[kIDpos + nd++] = k + np;
+      xi[kIDcnt] = nd;
+      B->kstart = k;
+      B->kw = np;
+      B->k = k + np;
+      B->pending = nd;
+      B->npos += npos;
+      B->nneg += nneg;
+      B->flops += flops;
+      atomicAdd(s.flops + 1, flops);
+      atomicAdd(s.flops + 5, 1.0);
+      if (np < acc) atomicAdd(s.flops + 6, 1.0);
+      atomicAdd(s.flops + 7, (double)(nd - (np < acc ? 1 : 0)));
+      // the next panel's column maxima, filled by the trailing update
+      for (int j = 0; j < kBlk; j++) X[kXNext + j] = 0.0;
+      B->state = (nd == 0 && k + np >= ncand) ? 1 : 0;
     }
-    ncand--;
-    __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    B->ncand = ncand;
-    B->pending = 0;
-    if (B->k >= B->ncand) B->state = 2;
-  }
+  __syncthreads();
 }
 
-__global__ void app_open_kernel(DevState s, const int* __restrict__ list, int count) {
-  int open = 0, rem = 0;
-  for (int i = threadIdx.x; i < count; i += blockDim.x) {
-    const BigFront& B = s.big[list[i]];
-    if (B.state != 2) {
-      open++;
-      rem = max(rem, B.ncand - B.k);
+// ---------------------------------------------------------------- phase U
+
+// One 64 x 64 lower tile (I, J) of front B's trailing matrix, rank-kw update
+// with the panel's L (columns kstart..kstart+kw of F) and W (Wg).
+__device__ void phase_u_tile(const DevState& s, const BigFront& B, int I, int J, UpdSm& sm) {
+  const int tid = threadIdx.x;
+  const int tx = tid & 15;
+  const int ty = tid >> 4;
+  const int f = B.f;
+  const int k = B.k;
+  const int kw = B.kw;
+  const int ks = B.kstart;
+  double* F = s.dpool + B.doff;
+  const double* W = s.dpool + B.woff;
+  const int i0 = k + I * kTileU;
+  const int j0 = k + J * kTileU;
+  double cur[4][4];
+#pragma unroll
+  for (int b = 0; b < 4; b++) {
+    const int j = j0 + ty + 16 * b;
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      const int i = i0 + tx + 16 * a;
+      cur[a][b] = (j < f && i < f && i >= j) ? F[i + (size_t)f * j] : 0.0;
     }
   }
-  atomicAdd(s.big_meta + 19, open);
-  atomicMax(s.big_meta + 20, rem);
+  {
+    constexpr int kPer = kBigPanelMax * kTileU / kThreads;
+    double pa[kPer], pb[kPer];
+#pragma unroll
+    for (int q = 0; q < kPer; q++) {
+      const int e = tid + kThreads * q;
+      const int c = e / kTileU;
+      const int rr = e - c * kTileU;
+      pa[q] = 0.0;
+      pb[q] = 0.0;
+      if (c < kw) {
+        if (i0 + rr < f) pa[q] = F[i0 + rr + (size_t)f * (ks + c)];
+        if (j0 + rr < f) pb[q] = W[(size_t)c * f + j0 + rr];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kPer; q++) {
+      const int e = tid + kThreads * q;
+      const int c = e / kTileU;
+      const int rr = e - c * kTileU;
+      if (c < kw) {
+        sm.As[c][rr] = pa[q];
+        sm.Bs[c][rr] = pb[q];
+      }
+    }
+  }
+  __syncthreads();
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) acc[a][b] = 0.0;
+  for (int c = 0; c < kw; c++) {
+    double av[4], bv[4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) av[a] = sm.As[c][tx + 16 * a];
+#pragma unroll
+    for (int b = 0; b < 4; b++) bv[b] = sm.Bs[c][ty + 16 * b];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+  }
+#pragma unroll
+  for (int b = 0; b < 4; b++) {
+    const int j = j0 + ty + 16 * b;
+    if (j >= f) continue;
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+      const int i = i0 + tx + 16 * a;
+      if (i < f && i >= j) F[i + (size_t)f * j] = cur[a][b] - acc[a][b];
+    }
+  }
+  if (J == 0) {
+    // the next panel's columns [k, k + 32): their largest magnitude over the
+    // rows below the next block, for its first test (the 16 threads with
+    // the same ty are one half-warp)
+    unsigned long long* nxt =
+        reinterpret_cast<unsigned long long*>(s.dpool + B.xoff + kAppNextColmax);
+#pragma unroll
+    for (int b = 0; b < 2; b++) {
+      double m = 0.0;
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const int i = i0 + tx + 16 * a;
+        if (i < f && i >= k + kBigPanelMax) m = fmax(m, fabs(cur[a][b] - acc[a][b]));
+      }
+#pragma unroll
+      for (int o = 1; o < 16; o <<= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      const int j = j0 + ty + 16 * b;
+      if (tx == 0 && j < f && m > 0.0)
+        atomicMax(nxt + (ty + 16 * b), (unsigned long long)__double_as_longlong(m));
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ long long tri_tiles(const BigFront& B) {
+  const long long t = (B.f - B.k + kTileU - 1) / kTileU;
+  return t * (t + 1) / 2;
+}
+
+// ---------------------------------------------------------------- the level
+
+__global__ void __launch_bounds__(kThreads, 1)
+    app_level_kernel(DevState s, FactorParams prm, const int* __restrict__ list, int nl,
+                     int max_steps, int* counters) {
+  cg::grid_group grid = cg::this_grid();
+  extern __shared__ __align__(16) unsigned char dsm[];
+  __shared__ Prefix P;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int gwarp = blockIdx.x * kWarps + warp;
+  const int nwarp = gridDim.x * kWarps;
+  int step = 1;
+  for (; step <= max_steps; step++) {
+    // ---- D: one warp per front
+    {
+      WarpDiag& w = reinterpret_cast<WarpDiag*>(dsm)[warp];
+      if (blockIdx.x == 0 && tid == 0) counters[(step + 1) & 1] = 0;
+      for (int i = gwarp; i < nl; i += nwarp) {
+        const int on = phase_d_front(s, prm, s.big + list[i], step, w);
+        if (on && (tid & 31) == 0) atomicAdd(counters + (step & 1), 1);
+      }
+    }
+    grid.sync();
+    if (*((volatile int*)(counters + (step & 1))) == 0) break;  // the same in every CTA
+    // ---- R: row chunks of the active fronts
+    for (int c0 = 0; c0 < nl; c0 += kChunkFronts) {
+      const int n = min(kChunkFronts, nl - c0);
+      const long long total = front_prefix(
+          P, n, [&](int i) { return (long long)row_chunks(s, s.big[list[c0 + i]], step); });
+      RowsSm& sm = *reinterpret_cast<RowsSm*>(dsm);
+      for (long long t = blockIdx.x; t < total; t += gridDim.x) {
+        const int fi = item_front(P, n, t);
+        const BigFront& B = s.big[list[c0 + fi]];
+        const int nchunk = (int)(P.ptr[fi + 1] - P.ptr[fi]);
+        phase_r_item(s, B, (int)(t - P.ptr[fi]), nchunk, sm);
+      }
+      __syncthreads();
+    }
+    grid.sync();
+    // ---- A: the same items; the first one of a front commits the panel
+    for (int c0 = 0; c0 < nl; c0 += kChunkFronts) {
+      const int n = min(kChunkFronts, nl - c0);
+      const long long total = front_prefix(
+          P, n, [&](int i) { return (long long)row_chunks(s, s.big[list[c0 + i]], step); });
+      RowsSm& sm = *reinterpret_cast<RowsSm*>(dsm);
+      for (long long t = blockIdx.x; t < total; t += gridDim.x) {
+        const int fi = item_front(P, n, t);
+        phase_a_item(s, prm, s.big + list[c0 + fi], (int)(t - P.ptr[fi]), sm);
+      }
+      __syncthreads();
+    }
+    grid.sync();
+    // ---- U: trailing-update tiles of the fronts that accepted pivots
+    for (int c0 = 0; c0 < nl; c0 += kChunkFronts) {
+      const int n = min(kChunkFronts, nl - c0);
+      const long long total = front_prefix(P, n, [&](int i) {
+        const BigFront& B = s.big[list[c0 + i]];
+        return (active(s, B, step) && B.kw > 0) ? tri_tiles(B) : 0ll;
+      });
+      UpdSm& sm = *reinterpret_cast<UpdSm*>(dsm);
+      for (long long t = blockIdx.x; t < total; t += gridDim.x) {
+        const int fi = item_front(P, n, t);
+        const BigFront& B = s.big[list[c0 + fi]];
+        const long long lt = t - P.ptr[fi];
+        int I = (int)((sqrt(8.0 * (double)lt + 1.0) - 1.0) * 0.5);
+        while ((long long)(I + 1) * (I + 2) / 2 <= lt) I++;
+        while ((long long)I * (I + 1) / 2 > lt) I--;
+        const int J = (int)(lt - (long long)I * (I + 1) / 2);
+        phase_u_tile(s, B, I, J, sm);
+      }
+      __syncthreads();
+    }
+    grid.sync();
+  }
+  // the step cap (never reached when every step makes progress)
+  if (step > max_steps && blockIdx.x == 0 && tid == 0) counters[2] = 1;
 }
 
 }  // namespace
 
-cudaError_t launch_app_panel(const DevState& s, const FactorParams& prm, int count, int max_f,
-                             const int* list, int step, cudaStream_t stream) {
+cudaError_t launch_app_level(const DevState& s, const FactorParams& prm, int count, int max_fs,
+                             const int* list, int* counters, cudaStream_t stream) {
   static_assert(kBlk == kBigPanelMax, "panel width");
   if (count <= 0) return cudaSuccess;
-  const int ych = std::max(1, std::min(64, (max_f + kRowThreads - 1) / kRowThreads));
-  app_diag_kernel<<<count, 128, 0, stream>>>(s, prm, list, step);
-  app_rows_kernel<<<dim3(count, ych), kRowThreads, 0, stream>>>(s, list, step);
-  app_accept_kernel<<<dim3(count, ych), kRowThreads, 0, stream>>>(s, prm, list, step);
-  return cudaGetLastError();
+  int dev = 0, nsm = 0, per = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, app_level_kernel, kThreads, kDynSmem);
+  if (e != cudaSuccess) return e;
+  if (per < 1) return cudaErrorLaunchOutOfResources;
+  const int grid = nsm * per;
+  // every step of an active front accepts a pivot or delays a candidate
+  int max_steps = max_fs + 8;
+  DevState sa = s;
+  FactorParams pa = prm;
+  const int* la = list;
+  int na = count;
+  int* ca = counters;
+  void* args[] = {(void*)&sa, (void*)&pa, (void*)&la, (void*)&na, (void*)&max_steps, (void*)&ca};
+  return cudaLaunchCooperativeKernel((const void*)app_level_kernel, dim3(grid), dim3(kThreads),
+                                     args, kDynSmem, stream);
 }
 
-cudaError_t launch_app_delay(const DevState& s, int count, const int* list, int step,
-                             cudaStream_t stream) {
-  if (count <= 0) return cudaSuccess;
-  app_delay_kernel<<<count, 256, 0, stream>>>(s, list, step);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_app_open_count(const DevState& s, int count, const int* list,
-                                  cudaStream_t stream) {
-  if (count <= 0) return cudaSuccess;
-  app_open_kernel<<<1, 256, 0, stream>>>(s, list, count);
-  return cudaGetLastError();
+cudaError_t configure_app_kernels() {
+  return cudaFuncSetAttribute(app_level_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)kDynSmem);
 }
 
 }  // namespace b200ldl

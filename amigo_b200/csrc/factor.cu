@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kFactorThreads)
       // on-chip limit also get the chained panel's W by physical row and its
       // permutation scratch
       unsigned long long need = (unsigned long long)f * f + (unsigned long long)kBigPanelMax * f;
-      if (prm.app && nc > 0)
+      if (prm.app && nc > 0 && f >= prm.app_min_f)
         need += (unsigned long long)kAppScratch;
       else if (f > s.cf_limit[4])
         need += (unsigned long long)kBigPanelMax * f + (unsigned long long)(fs + 1) * f;
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(kFactorThreads)
       const int slot = atomicAdd(s.big_meta, 1);
       atomicMax(s.big_meta + 1, f);
       atomicMax(s.big_meta + 2, fs);
-      const bool app = prm.app && nc > 0;
+      const bool app = prm.app && nc > 0 && f >= prm.app_min_f;
       int cls = 5;
       if (app) {
         cls = 6;

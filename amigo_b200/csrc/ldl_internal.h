@@ -157,7 +157,7 @@ struct DevState {
   int* big_meta;    // [kBigMeta]: count, max f, max fs, count large, max fs
                     // large, class counts [5..9], class max f [10..14], max f
                     // large [15], a-posteriori fronts: count [16], max f [17],
-                    // max fs [18], not yet done [19], most candidates left [20]
+                    // max fs [18], their step counters and cap flag [21..23]
   int* class_list;  // [7][nn] big-front indices per size class (6: a-posteriori)
   int cf_limit[5];  // largest front of each on-chip class
   // fronts re-planned from a pivot record: partner[v] = the variable that
@@ -172,8 +172,10 @@ struct FactorParams {
   int cholesky;
   // fronts above the shared-memory limit that have contribution rows are
   // factored in blocked panels with a-posteriori threshold tests
-  // (big_app.cu) instead of the candidate-by-candidate search
+  // (big_app.cu) instead of the candidate-by-candidate search, from fronts
+  // of app_min_f rows up
   int app;
+  int app_min_f;
 };
 
 // Largest front factored entirely in shared memory (fp64, ld = f | 1).
@@ -216,19 +218,14 @@ cudaError_t configure_big_chain_kernel();
 cudaError_t launch_big_chain_panel(const DevState& s, const FactorParams& prm, int count,
                                    int max_f, int nb, const int* list, cudaStream_t stream);
 
-// A-posteriori blocked panels (big_app.cu) for the class-6 fronts in
-// `list`: one panel step (diagonal block, rows below and tests, accepted
-// columns), and the delay of a candidate whose test failed (after the
-// trailing update of the step). `step` numbers the steps of one level from 1
-// up; the panel state is stamped with it.
-cudaError_t launch_app_panel(const DevState& s, const FactorParams& prm, int count, int max_f,
-                             const int* list, int step, cudaStream_t stream);
-cudaError_t launch_app_delay(const DevState& s, int count, const int* list, int step,
-                             cudaStream_t stream);
-// number of class-6 fronts not yet done into s.big_meta[19], the most
-// candidates any of them has left into s.big_meta[20]
-cudaError_t launch_app_open_count(const DevState& s, int count, const int* list,
-                                  cudaStream_t stream);
+// A-posteriori blocked panels (big_app.cu): every panel step of the class-6
+// fronts in `list` (count of them, the largest with max_fs candidates) in
+// one cooperative launch. counters: 3 zeroed ints in device memory;
+// counters[2] is set if the step cap was reached (it is not when every step
+// makes progress).
+cudaError_t launch_app_level(const DevState& s, const FactorParams& prm, int count, int max_fs,
+                             const int* list, int* counters, cudaStream_t stream);
+cudaError_t configure_app_kernels();
 
 cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
                              int maxkids, const FactorParams& prm, const double* vals,
