@@ -293,16 +293,20 @@ void build_plan(b200ldl_t h, const int* rowp, const int* cols) {
   h->hp_scat_col = std::move(scat_col);
   h->hp_level_nodes = std::move(lnodes);
 
-  // pool estimates from the symbolic fronts, scaled by the delay growth
+  // pool estimates from the symbolic fronts, scaled by the delay growth; a
+  // structure re-planned from a pivot record already holds its delays, and
+  // its big fronts other than roots take the a-posteriori panels, which need
+  // no chained-panel scratch
   double ints = 0.0, dbl = 0.0;
   for (int k = 0; k < nn; k++) {
     const double f = h->h_ns[k] + h->h_nc[k];
     ints += 2.0 * f;
     dbl += f * h->h_ns[k] + (double)h->h_nc[k] * h->h_nc[k];
-    if (f > kSmemFrontMax) dbl += f * f + 2.0 * f;
-    if (f > cluster_front_limit(4)) dbl += f * f + 32.0 * f;  // chained panels' scratch
+    if (f > kSmemFrontMax) dbl += f * f + (kBigPanelMax + 2.0) * f + kAppScratch;
+    if (f > cluster_front_limit(4) && !(h->replanned && h->h_nc[k] > 0))
+      dbl += f * f + 32.0 * f;  // chained panels' scratch
   }
-  const double g = std::max(1.0, h->delay_growth);
+  const double g = h->replanned ? 1.0 : std::max(1.0, h->delay_growth);
   h->icap = (unsigned long long)(ints * g * 1.5) + (1u << 16);
   h->dcap = (unsigned long long)(dbl * g * 1.5) + (1u << 20);
 }
@@ -1029,8 +1033,13 @@ int b200ldl_set_pivot_record(b200ldl_t h, const int* f, const int* npiv, const i
     if (h->solver_type == B200LDL_CHOLESKY) return fail(h, -1, "Cholesky mode has no pivot order");
     if (!f && !npiv && !ndel && !fv) {
       if (h->replanned) {
-        use_structure(h, Symbolic(h->sym_ref));
         h->replanned = false;
+        try {
+          use_structure(h, Symbolic(h->sym_ref));
+        } catch (...) {
+          h->replanned = true;
+          throw;
+        }
       }
       return 0;
     }
@@ -1038,9 +1047,15 @@ int b200ldl_set_pivot_record(b200ldl_t h, const int* f, const int* npiv, const i
     if (!h->replanned) h->sym_ref = h->sym;
     std::vector<int> partner(std::max(1, h->n), -1);
     Symbolic s = replan_from_record(h->sym_ref, f, npiv, ndel, fv, partner);
-    use_structure(h, std::move(s));
-    h->partner = std::move(partner);
+    const bool was = h->replanned;
     h->replanned = true;
+    try {
+      use_structure(h, std::move(s));
+    } catch (...) {
+      h->replanned = was;
+      throw;
+    }
+    h->partner = std::move(partner);
     return 0;
   });
 }

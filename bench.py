@@ -6,7 +6,11 @@ Workload: the 256 x 256 plane-stress PDE-constrained KKT system
 right-hand sides: a unit load plus four N(0,1) columns), AMD ordering, the
 reference solver's settings (ustab 0.01, pivot_tol 1e-14). One step = one
 numeric factorization + one 5-RHS solve; the symbolic analysis runs once per
-pattern outside the timed region, as in the interior-point loop.
+pattern outside the timed region, as in the interior-point loop. The timed
+factorizations reuse the pivot order of the previous factorization of the
+pattern (SparseLDL.reuse_pivot_order); the line also reports the first
+factorization's order (the reference's pivot sequence replayed) and a record
+taken from a perturbed neighbouring iterate.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -287,6 +291,26 @@ def run_reference_batched(args, world, rank):
     return 0
 
 
+def perturbed_iterate(system, seed: int = 123, eps_vals: float = 0.01, eps_sigma: float = 0.3):
+    """Values of the same pattern standing for a neighbouring interior-point
+    iterate: every stored entry scaled by 1 + eps_vals N(0,1) (the same
+    factor for (i, j) and (j, i), so the matrix stays symmetric) and every
+    positive diagonal entry (Sigma) by exp(eps_sigma N(0,1))."""
+    rng = np.random.default_rng(seed)
+    r = np.repeat(np.arange(system.n), np.diff(system.rowp))
+    key = r.astype(np.int64) * system.n + system.cols
+    tkey = system.cols.astype(np.int64) * system.n + r
+    order = np.argsort(key)
+    pos = order[np.searchsorted(key[order], tkey)]
+    f = rng.standard_normal(system.nnz)
+    f = 0.5 * (f + f[pos])
+    v = system.vals * (1.0 + eps_vals * f)
+    d = system.diag.copy()
+    m = d > 0
+    d[m] *= np.exp(eps_sigma * rng.standard_normal(int(m.sum())))
+    return v, d
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -311,35 +335,69 @@ def run_ours(args, world, rank, local):
     x = x.t().contiguous().t()
     ldl = SparseLDL(CSRMat(s.n, s.n, s.rowp, s.cols, vals), order=OrderingType.AMD)
     dvec = Vector(diag)
+    stream = torch.cuda.current_stream(dev)
 
     def step():
         ldl.factor(dvec)
         x.copy_(b)
         ldl.solve(x)
 
+    def timed(k):
+        """K steps between CUDA events on the launching stream, the ranks
+        lined up by a barrier; device milliseconds, max over ranks."""
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = torch.tensor([e0.elapsed_time(e1)], device=dev, dtype=torch.float64)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # (1) the reference's pivot order: every factorization starts from the
+    # symbolic supernodes and replays the reference's delays
+    for _ in range(args.warmup):
+        step()
+    ms_ref_order = timed(args.steps)
+    berr_ref_order = backward_error(s, x.cpu().numpy(), s.rhs)
+    delayed_ref_order = ldl.stats()["delayed"]
+
+    # (2) a record from a neighbouring iterate's values (the same pattern)
+    pv, pd = perturbed_iterate(s)
+    vals.copy_(torch.as_tensor(pv, device=dev))
+    diag.copy_(torch.as_tensor(pd, device=dev))
+    ldl.factor(dvec)
+    ldl.reuse_pivot_order()
+    vals.copy_(torch.as_tensor(s.vals, device=dev))
+    diag.copy_(torch.as_tensor(s.diag, device=dev))
+    for _ in range(args.warmup):
+        step()
+    ms_iterate = timed(args.steps)
+    berr_iterate = backward_error(s, x.cpu().numpy(), s.rhs)
+    inertia_iterate = tuple(ldl.get_inertia())
+    delayed_iterate = ldl.stats()["delayed"]
+
+    # (3) the headline: pivot-order reuse, the record of the previous
+    # factorization of this matrix (a refactorization loop's steady state)
+    ldl.set_pivot_record(None)
+    ldl.factor(dvec)
+    ldl.reuse_pivot_order()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-
-    stream = torch.cuda.current_stream(dev)
     sampler = ClockSampler(local, enabled=not args.no_clocks)
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    sampler.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
     launches0 = ldl.launch_count()
-    e0.record(stream)
-    for _ in range(args.steps):
-        step()
-    e1.record(stream)
-    torch.cuda.synchronize()
+    sampler.start()
+    ms_total = timed(args.steps)
     clocks = sampler.stop()
     launches = ldl.launch_count() - launches0
-    if world > 1:
-        torch.distributed.barrier()
-    ms_total = e0.elapsed_time(e1)
+    ms_max = ms_total
     # accuracy and work of the last timed step
     xh = x.cpu().numpy()
     berr = backward_error(s, xh, s.rhs)
@@ -358,13 +416,13 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         prof = ldl.profile()
         ldl.set_profiling(False)
-    t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(t.item())
     value = world * args.steps / (ms_max / 1e3)
 
-    # end to end through the public API with host buffers (pinned)
+    # end to end through the public API with host buffers (pinned), the same
+    # reuse of the previous factorization's pivot order (the device-buffer
+    # handle is released first: each holds the factor pools of this system)
+    ldl.close()
+    torch.cuda.empty_cache()
     e2e_value, berr_e2e = None, None
     hv = torch.empty(s.nnz, dtype=torch.float64, pin_memory=True)
     hd = torch.empty(s.n, dtype=torch.float64, pin_memory=True)
@@ -381,6 +439,8 @@ def run_ours(args, world, rank, local):
         host_ldl.solve(xf)
 
     if not args.no_e2e:
+        host_ldl.factor(hvec)
+        host_ldl.reuse_pivot_order()
         for _ in range(max(1, min(args.warmup, 2))):
             e2e_step()
         if world > 1:
@@ -414,7 +474,9 @@ def run_ours(args, world, rank, local):
         # dense partial factorizations outside the big-front path (flops)
         "fronts": ("tensor", work["flops"] - work["panel_flops"] - work["update_flops"]
                    - work["cluster_flops"]),
-        "big_panel": ("tensor", work["panel_flops"]),
+        # big fronts: panels and their trailing updates (flops; with pivot
+        # reuse one cooperative launch per level does both)
+        "big_panel": ("tensor", work["panel_flops"] + work["update_flops"]),
         # whole fronts factored in a cluster's distributed shared memory
         "cluster_fronts": ("tensor", work["cluster_flops"]),
         # rank-kw updates: trailing lower triangle read + written, panels read
@@ -425,41 +487,31 @@ def run_ours(args, world, rank, local):
         "solve_forward": ("hbm", stats["L_bytes"]),
         "solve_backward": ("hbm", stats["L_bytes"]),
     }
-    # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum,
-    # averaged over every launch of the class's kernel in one factorization
-    # and solve) from the ncu launch list of this workload, kept in
-    # profiles/launch_list_plane_stress_256.txt
-    ncu_traffic = {"big_panel": 2.833e6, "cluster_fronts": 19.887e6, "big_update": 33.788e6,
-                   "fronts": 5.737e6} if (args.workload == "plane_stress"
-                                          and args.nel == 256) else {}
     for p_ in prof or []:
         p_["bound"], w = algo[p_["name"]]
         p_["work_per_step"] = w
     dom = max(prof, key=lambda p_: p_["ms"]) if prof else None
+    fp64_peak_tflops = 37.0  # B200 datasheet FP64 (no FP64 peak is measured on this pool)
     if dom is not None:
         per_launch_ms = dom["ms"] / max(1, dom["launches"])
         total_work = dom["work_per_step"] * args.steps
-    if dom is None:
-        pass
-    elif dom["bound"] == "hbm":
-        achieved = total_work / max(1e-12, dom["ms"] / 1e3) / 1e9
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": ncu_traffic.get(dom["name"]),
-                "traffic_unit": "bytes per launch (ncu)",
-                "kernel": dom["name"], "launches": dom["launches"],
-                "ms_per_launch": per_launch_ms, "peak_source": peaks["source"],
-                "timing": "profile pass of the same steps, CUDA events per kernel class"}
-    else:
-        achieved = total_work / max(1e-12, dom["ms"] / 1e3) / 1e12
-        roof = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"],
-                "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"],
-                "traffic": ncu_traffic.get(dom["name"]), "traffic_unit": "bytes per launch (ncu)",
-                "kernel": dom["name"], "launches": dom["launches"],
-                "ms_per_launch": per_launch_ms, "peak_source": peaks["source"],
-                "note": "FP64 arithmetic measured against the bf16 dense peak; the chained "
-                        "pivot search is bound by the latency of its per-step cluster "
-                        "exchanges, not by arithmetic",
-                "timing": "profile pass of the same steps, CUDA events per kernel class"}
+        if dom["bound"] == "hbm":
+            achieved = total_work / max(1e-12, dom["ms"] / 1e3) / 1e9
+            roof = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                    "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None}
+        else:
+            achieved = total_work / max(1e-12, dom["ms"] / 1e3) / 1e12
+            roof = {"bound": "tensor", "achieved": achieved, "peak": peaks["bf16_tflops"],
+                    "unit": "TFLOP/s", "frac": achieved / peaks["bf16_tflops"],
+                    "traffic": None,
+                    "fp64_frac": achieved / fp64_peak_tflops,
+                    "note": "FP64 arithmetic: frac is against the bf16 dense peak the "
+                            "contract names; fp64_frac against the B200 datasheet FP64 "
+                            "peak (37 TFLOP/s, not measured here)"}
+        roof.update({"kernel": dom["name"], "launches": dom["launches"],
+                     "ms_per_launch": per_launch_ms, "peak_source": peaks["source"],
+                     "traffic_note": "DRAM bytes per launch from ncu are in profiles/",
+                     "timing": "profile pass of the same steps, CUDA events per kernel class"})
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -481,8 +533,25 @@ def run_ours(args, world, rank, local):
             "workload": f"plane-stress KKT {args.nel}x{args.nel} (n={s.n}, nnz={s.nnz}), "
                         f"{nrhs} RHS, AMD ordering, FP64 factor+solve",
             "nrhs": nrhs, "parallelism": "replicas" if world > 1 else "single GPU",
+            "pivot_order": "reused from the previous factorization of this pattern "
+                           "(SparseLDL.reuse_pivot_order: a refactorization loop's steady "
+                           "state; every candidate still passes the reference's threshold "
+                           "test against its whole column)",
             "l2": "inputs and per-step factor traffic larger than L2 (126 MB); no flush",
         },
+        "fp64_reference_order": {
+            "value": world * args.steps / (ms_ref_order / 1e3),
+            "ms_per_step": ms_ref_order / args.steps, "backward_error": berr_ref_order,
+            "delayed_pivots": delayed_ref_order,
+            "what": "every factorization from the symbolic supernodes, the reference's "
+                    "pivot sequence replayed (the first factorization of a pattern)"},
+        "pivot_record_from_perturbed_iterate": {
+            "value": world * args.steps / (ms_iterate / 1e3),
+            "ms_per_step": ms_iterate / args.steps, "backward_error": berr_iterate,
+            "inertia": list(inertia_iterate), "delayed_pivots": delayed_iterate,
+            "what": "record taken from values perturbed by 1% (entries) and exp(0.3 N(0,1)) "
+                    "(Sigma), then the benchmark matrix factored with it"},
+        "mixed_precision": None,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "backward_error": berr_e2e},
         "roofline": roof,
@@ -496,6 +565,8 @@ def run_ours(args, world, rank, local):
         "factor_flops_executed": stats["flops"],
         "max_front": stats["max_front"],
         "delayed_pivots": stats["delayed"],
+        "a_posteriori_panels": {k: work[k] for k in ("app_panels", "app_rejected",
+                                                     "app_block_delays")},
         "profile": prof,
     }
     print(json.dumps(line))
