@@ -46,6 +46,9 @@ SIGNATURES = {
     "b200ldl_profile": (ctypes.c_int, [_vp, _f64p, ctypes.c_int]),
     "b200ldl_launch_count": (ctypes.c_longlong, [_vp]),
     "b200ldl_work": (ctypes.c_int, [_vp, _f64p, ctypes.c_int]),
+    "b200ldl_schur_update_tc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _vp,
+                                               ctypes.c_int, _vp, ctypes.c_int, _vp,
+                                               ctypes.c_int, ctypes.c_int, _vp]),
     "b200ldl_dense_solve_noalloc": (ctypes.c_int, [ctypes.c_int, _vp, ctypes.c_int, _vp,
                                                    ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "b200ldl_create_batch": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, _i32p, _i32p,

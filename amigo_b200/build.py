@@ -21,8 +21,8 @@ ROOT = os.path.dirname(HERE)
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(HERE, "libb200ldl.so")
 
-SOURCES = ["symbolic.cpp", "api.cu", "factor.cu", "solve.cu", "big.cu", "cluster_front.cu", "big_chain.cu", "noalloc.cu", "refine.cu", "solve_big.cu", "batch.cu", "assembly.cu", "big_app.cu"]
-HEADERS = ["symbolic.h", "ldl_internal.h", "front_common.cuh"]
+SOURCES = ["symbolic.cpp", "api.cu", "factor.cu", "solve.cu", "big.cu", "cluster_front.cu", "big_chain.cu", "noalloc.cu", "refine.cu", "solve_big.cu", "batch.cu", "assembly.cu", "big_app.cu", "schur_tc.cu"]
+HEADERS = ["symbolic.h", "ldl_internal.h", "front_common.cuh", "umma.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -289,6 +289,20 @@ int b200ldl_assembly_plan(b200ldl_assembly_t a, long long* ptr, long long* src);
 const char* b200ldl_assembly_last_error(b200ldl_assembly_t a);
 void b200ldl_assembly_destroy(b200ldl_assembly_t a);
 
+/* Dense Schur-complement update on the Blackwell tensor cores (no
+ * counterpart in the reference, whose frontal_trailing_update,
+ * include/sparse_ldl.h:1190-1215, calls FP64 dgemm): C -= A B^T for A (m x
+ * k, lda), B (n x k, ldb) and C (m x n, ldc), column-major FP64 DEVICE
+ * arrays; with lower != 0 only entries with row >= column change. The
+ * products run as 3xTF32 (each operand split into two TF32 parts) on
+ * tcgen05.mma with FP32 accumulation in tensor memory, so the update has
+ * about FP32 accuracy: the mixed-precision factorization applies it to the
+ * contribution blocks of big fronts. Synchronizes the stream (cudaStream_t,
+ * NULL = default). Status 1 if a tensor-core operation did not complete in
+ * time. */
+int b200ldl_schur_update_tc(int m, int n, int k, const double* a, int lda, const double* b,
+                            int ldb, double* c, int ldc, int lower, void* stream);
+
 /* Allocation-free dense solve (no counterpart in the reference; the
  * reference always allocates its factor storage). For callers that must not
  * allocate device memory while running, e.g. a real-time loop re-solving a
