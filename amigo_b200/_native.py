@@ -32,6 +32,9 @@ SIGNATURES = {
                                             ctypes.c_int, ctypes.c_int, ctypes.c_double, _f64p,
                                             _i32p]),
     "b200ldl_get_inertia": (ctypes.c_int, [_vp, _i32p, _i32p]),
+    "b200ldl_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "b200ldl_set_refinement": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double]),
+    "b200ldl_last_refinement": (ctypes.c_int, [_vp, _i32p, _f64p, _i32p, _i32p]),
     "b200ldl_last_error": (ctypes.c_char_p, [_vp]),
     "b200ldl_symbolic_sizes": (ctypes.c_int, [_vp, _i32p, _i32p]),
     "b200ldl_get_symbolic": (ctypes.c_int, [_vp] + [_i32p] * 7),

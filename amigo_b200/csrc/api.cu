@@ -83,6 +83,21 @@ struct b200ldl_handle {
   // 2x2 partners of the pivot record the structure was re-planned from
   std::vector<int> partner;
   DevBuf<int> d_partner;
+  // precision of the big fronts' contribution-block updates; in MIXED mode
+  // every solve is refined in FP64 against the matrix of the last factor
+  int precision = B200LDL_FP64;
+  int refine_max = 5;
+  double refine_tol = 1e-12;
+  bool factored_mixed = false;
+  const double* last_vals = nullptr;
+  const double* last_diag = nullptr;
+  int last_iters = 0;
+  double last_berr = 0.0;
+  // inertia of the last FP64 factorization (-1: none yet), against which a
+  // mixed factorization is checked, and the FP64 redos the checks caused
+  int fp64_inertia[2] = {-1, -1};
+  int mixed_fallbacks = 0;
+  DevBuf<double> d_rhs_tmp;
   bool uploaded = false;
   // independent systems factored as one forest (1 for a single system)
   int nsys = 1;
@@ -503,13 +518,17 @@ void configure_device_kernels() {
   done[dev] = 1;
 }
 
-void run_factor(b200ldl_t h, const double* vals, const double* diag) {
+void run_factor_once(b200ldl_t h, const double* vals, const double* diag, bool mixed) {
   configure_device_kernels();
   // fronts re-planned from a pivot record are expected to accept their
   // candidates where they stand: their big fronts take the blocked panels
   // with a-posteriori tests
   FactorParams prm{h->ustab, h->pivot_tol, h->solver_type == B200LDL_CHOLESKY ? 1 : 0,
-                   (h->replanned && h->solver_type != B200LDL_CHOLESKY) ? 1 : 0, 0};
+                   (h->replanned && h->solver_type != B200LDL_CHOLESKY) ? 1 : 0, 0, 0};
+  prm.mixed = (prm.app && mixed) ? 1 : 0;
+  h->factored_mixed = prm.mixed != 0;
+  h->last_vals = vals;
+  h->last_diag = diag;
   for (int attempt = 0; attempt < 12; attempt++) {
     ensure_pools(h);
     CK(cudaMemsetAsync(h->d_used.ptr, 0, 3 * sizeof(unsigned long long), h->stream));
@@ -590,6 +609,27 @@ void run_factor(b200ldl_t h, const double* vals, const double* diag) {
     h->dcap = std::max<unsigned long long>(h->dcap * 2, h->used[1] + (1u << 20));
   }
   throw std::runtime_error("factor storage did not converge after repeated growth");
+}
+
+// A mixed-precision factorization is kept only if its inertia equals that of
+// the last FP64 factorization of the pattern (the one whose pivot record the
+// handle reuses, or a later one); otherwise, and whenever no FP64 inertia is
+// known yet, the factorization runs in FP64. Rounding at FP32 level in the
+// contribution blocks can flip the sign of a pivot that cancellation makes
+// tiny, so the FP64 factorization decides the inertia in that case.
+void run_factor(b200ldl_t h, const double* vals, const double* diag) {
+  const bool mixed = h->replanned && h->precision == B200LDL_MIXED &&
+                     h->solver_type != B200LDL_CHOLESKY && h->fp64_inertia[0] >= 0;
+  if (mixed) {
+    run_factor_once(h, vals, diag, true);
+    if (!h->factored_mixed || (h->inertia[0] == h->fp64_inertia[0] &&
+                               h->inertia[1] == h->fp64_inertia[1]))
+      return;
+    h->mixed_fallbacks++;
+  }
+  run_factor_once(h, vals, diag, false);
+  h->fp64_inertia[0] = h->inertia[0];
+  h->fp64_inertia[1] = h->inertia[1];
 }
 
 
@@ -675,6 +715,65 @@ int guarded(b200ldl_t h, F&& fn) {
   } catch (const std::exception& e) {
     return fail(h, -4, "%s", e.what());
   }
+}
+
+// x = K^-1 b with FP64 iterative refinement against the CSR values `vals`
+// and `diag` (device), every column until its backward error is <= tol or
+// max_iter corrections were made; berr_out (host, nrhs entries) may be null.
+void refine_impl(b200ldl_t h, const double* vals, const double* diag, int nrhs, const double* b,
+                 int ldb, double* x, int ldx, int max_iter, double tol, double* berr_out,
+                 int* iters_out) {
+    if (iters_out) *iters_out = 0;
+    if (nrhs == 0 || h->n == 0) return;
+    const int n = h->n;
+    const int chunk = refine_max_rhs();
+    if (h->d_refine.count < (size_t)n * chunk) CK(h->d_refine.alloc((size_t)n * chunk));
+    if (h->d_norms.count < (size_t)(1 + 3 * chunk)) CK(h->d_norms.alloc(1 + 3 * chunk));
+    double* r = h->d_refine.ptr;
+    double* nrm = h->d_norms.ptr;  // [0] ||K||, [1..] ||b||, ||x||, ||r|| per column
+    CK(cudaMemsetAsync(nrm, 0, sizeof(double), h->stream));
+    launch_infnorm(n, h->d_rowp.ptr, h->d_cols.ptr, vals, diag, nrm, h->stream);
+    int max_it_done = 0;
+    double worst = 0.0;
+    for (int c0 = 0; c0 < nrhs; c0 += chunk) {
+      const int nr = std::min(chunk, nrhs - c0);
+      const double* bc = b + (size_t)ldb * c0;
+      double* xc = x + (size_t)ldx * c0;
+      launch_copy_cols(n, nr, bc, ldb, xc, ldx, h->stream);
+      run_solve(h, nr, xc, ldx);
+      CK(cudaMemsetAsync(nrm + 1, 0, sizeof(double) * chunk, h->stream));
+      launch_colmax(n, bc, ldb, nr, nrm + 1, h->stream);
+      int it = 0;
+      for (;; it++) {
+        launch_residual(n, h->d_rowp.ptr, h->d_cols.ptr, vals, diag, xc, ldx, bc, ldb, r, n, nr,
+                        h->stream);
+        CK(cudaMemsetAsync(nrm + 1 + chunk, 0, sizeof(double) * 2 * chunk, h->stream));
+        launch_colmax(n, xc, ldx, nr, nrm + 1 + chunk, h->stream);
+        launch_colmax(n, r, n, nr, nrm + 1 + 2 * chunk, h->stream);
+        double hn[1 + 3 * 8];
+        CK(cudaMemcpyAsync(hn, nrm, sizeof(double) * (1 + 3 * chunk), cudaMemcpyDeviceToHost,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        bool ok = true;
+        for (int c = 0; c < nr; c++) {
+          const double den = hn[0] * hn[1 + chunk + c] + hn[1 + c];
+          const double be = den > 0.0 ? hn[1 + 2 * chunk + c] / den : 0.0;
+          if (berr_out) berr_out[c0 + c] = be;
+          worst = std::max(worst, be);
+          if (!(be <= tol)) ok = false;
+        }
+        if (ok || it >= max_iter) break;
+        run_solve(h, nr, r, n);
+        launch_axpy(n, nr, r, n, xc, ldx, h->stream);
+      }
+      max_it_done = std::max(max_it_done, it);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->stream));
+    h->prof.collect();
+    if (iters_out) *iters_out = max_it_done;
+    h->last_iters = max_it_done;
+    h->last_berr = worst;
 }
 
 }  // namespace
@@ -917,16 +1016,60 @@ int b200ldl_copy_perturbed_diagonal(b200ldl_t h, double* out) {
   });
 }
 
+// In place x <- K^-1 x for device x. After a mixed-precision factorization
+// the solution is refined in FP64 against the matrix that was factored.
+static void solve_inplace(b200ldl_t h, int nrhs, double* x, int ldx) {
+  if (h->factored_mixed && h->nnz > 0 && h->last_vals) {
+    const size_t cnt = (size_t)h->n * nrhs;
+    if (h->d_rhs_tmp.count < cnt) CK(h->d_rhs_tmp.alloc(cnt));
+    launch_copy_cols(h->n, nrhs, x, ldx, h->d_rhs_tmp.ptr, h->n, h->stream);
+    refine_impl(h, h->last_vals, h->last_diag, nrhs, h->d_rhs_tmp.ptr, h->n, x, ldx,
+                h->refine_max, h->refine_tol, nullptr, nullptr);
+    if (h->last_berr <= h->refine_tol) return;
+    // refinement stalled on the mixed factor: factor in FP64 and solve again
+    h->mixed_fallbacks++;
+    run_factor_once(h, h->last_vals, h->last_diag, false);
+    h->fmax = 0;
+    launch_copy_cols(h->n, nrhs, h->d_rhs_tmp.ptr, h->n, x, ldx, h->stream);
+  }
+  run_solve(h, nrhs, x, ldx);
+  CK(cudaStreamSynchronize(h->stream));
+  h->prof.collect();
+}
+
 int b200ldl_solve(b200ldl_t h, int nrhs, double* x, int ldx) {
   return guarded(h, [&]() {
     if (!h->factored) return fail(h, -5, "solve called before a successful factor");
     if (nrhs < 0 || ldx < h->n || (nrhs > 0 && !x)) return fail(h, -1, "bad solve arguments");
     if (nrhs == 0 || h->n == 0) return 0;
-    run_solve(h, nrhs, x, ldx);
-    CK(cudaStreamSynchronize(h->stream));
-    h->prof.collect();
+    solve_inplace(h, nrhs, x, ldx);
     return 0;
   });
+}
+
+int b200ldl_set_precision(b200ldl_t h, int mode) {
+  if (!h) return -1;
+  if (mode != B200LDL_FP64 && mode != B200LDL_MIXED) return fail(h, -1, "unknown precision mode");
+  h->precision = mode;
+  return 0;
+}
+
+int b200ldl_set_refinement(b200ldl_t h, int max_iter, double tol) {
+  if (!h) return -1;
+  if (max_iter < 0 || !(tol >= 0.0)) return fail(h, -1, "bad refinement settings");
+  h->refine_max = max_iter;
+  h->refine_tol = tol;
+  return 0;
+}
+
+int b200ldl_last_refinement(b200ldl_t h, int* iters, double* berr, int* mixed,
+                            int* fallbacks) {
+  if (!h) return -1;
+  if (iters) *iters = h->last_iters;
+  if (berr) *berr = h->last_berr;
+  if (mixed) *mixed = h->factored_mixed ? 1 : 0;
+  if (fallbacks) *fallbacks = h->mixed_fallbacks;
+  return 0;
 }
 
 int b200ldl_solve_host(b200ldl_t h, int nrhs, double* x, int ldx) {
@@ -937,7 +1080,7 @@ int b200ldl_solve_host(b200ldl_t h, int nrhs, double* x, int ldx) {
     const size_t cnt = (size_t)ldx * nrhs;
     if (h->d_x.count < cnt) CK(h->d_x.alloc(cnt));
     CK(cudaMemcpyAsync(h->d_x.ptr, x, cnt * sizeof(double), cudaMemcpyHostToDevice, h->stream));
-    run_solve(h, nrhs, h->d_x.ptr, ldx);
+    solve_inplace(h, nrhs, h->d_x.ptr, ldx);
     CK(cudaMemcpyAsync(x, h->d_x.ptr, cnt * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     h->prof.collect();
@@ -1103,53 +1246,7 @@ int b200ldl_solve_refine(b200ldl_t h, const double* vals, const double* diag, in
     if (nrhs < 0 || ldb < h->n || ldx < h->n || max_iter < 0 || (nrhs > 0 && (!b || !x)) ||
         (h->nnz > 0 && !vals))
       return fail(h, -1, "bad refine arguments");
-    if (iters_out) *iters_out = 0;
-    if (nrhs == 0 || h->n == 0) return 0;
-    const int n = h->n;
-    const int chunk = refine_max_rhs();
-    if (h->d_refine.count < (size_t)n * chunk) CK(h->d_refine.alloc((size_t)n * chunk));
-    if (h->d_norms.count < (size_t)(1 + 3 * chunk)) CK(h->d_norms.alloc(1 + 3 * chunk));
-    double* r = h->d_refine.ptr;
-    double* nrm = h->d_norms.ptr;  // [0] ||K||, [1..] ||b||, ||x||, ||r|| per column
-    CK(cudaMemsetAsync(nrm, 0, sizeof(double), h->stream));
-    launch_infnorm(n, h->d_rowp.ptr, h->d_cols.ptr, vals, diag, nrm, h->stream);
-    int max_it_done = 0;
-    for (int c0 = 0; c0 < nrhs; c0 += chunk) {
-      const int nr = std::min(chunk, nrhs - c0);
-      const double* bc = b + (size_t)ldb * c0;
-      double* xc = x + (size_t)ldx * c0;
-      launch_copy_cols(n, nr, bc, ldb, xc, ldx, h->stream);
-      run_solve(h, nr, xc, ldx);
-      CK(cudaMemsetAsync(nrm + 1, 0, sizeof(double) * chunk, h->stream));
-      launch_colmax(n, bc, ldb, nr, nrm + 1, h->stream);
-      int it = 0;
-      for (;; it++) {
-        launch_residual(n, h->d_rowp.ptr, h->d_cols.ptr, vals, diag, xc, ldx, bc, ldb, r, n, nr,
-                        h->stream);
-        CK(cudaMemsetAsync(nrm + 1 + chunk, 0, sizeof(double) * 2 * chunk, h->stream));
-        launch_colmax(n, xc, ldx, nr, nrm + 1 + chunk, h->stream);
-        launch_colmax(n, r, n, nr, nrm + 1 + 2 * chunk, h->stream);
-        double hn[1 + 3 * 8];
-        CK(cudaMemcpyAsync(hn, nrm, sizeof(double) * (1 + 3 * chunk), cudaMemcpyDeviceToHost,
-                           h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        bool ok = true;
-        for (int c = 0; c < nr; c++) {
-          const double den = hn[0] * hn[1 + chunk + c] + hn[1 + c];
-          const double be = den > 0.0 ? hn[1 + 2 * chunk + c] / den : 0.0;
-          if (berr_out) berr_out[c0 + c] = be;
-          if (!(be <= tol)) ok = false;
-        }
-        if (ok || it >= max_iter) break;
-        run_solve(h, nr, r, n);
-        launch_axpy(n, nr, r, n, xc, ldx, h->stream);
-      }
-      max_it_done = std::max(max_it_done, it);
-    }
-    CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(h->stream));
-    h->prof.collect();
-    if (iters_out) *iters_out = max_it_done;
+    refine_impl(h, vals, diag, nrhs, b, ldb, x, ldx, max_iter, tol, berr_out, iters_out);
     return 0;
   });
 }

@@ -56,6 +56,7 @@
 #include <climits>
 
 #include "ldl_internal.h"
+#include "umma.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -178,7 +179,12 @@ struct Prefix {  // work items of up to kChunkFronts fronts
 };
 
 constexpr size_t cmax(size_t a, size_t b) { return a > b ? a : b; }
-constexpr size_t kDynSmem = cmax(sizeof(WarpDiag) * kWarps, cmax(sizeof(RowsSm), sizeof(UpdSm)));
+// the mixed-precision tile places the tensor-core operands after the FP64
+// tiles' panels, 1 KB aligned
+constexpr size_t kOpsOffset = (sizeof(UpdSm) + 1023) / 1024 * 1024;
+constexpr size_t kDynSmem =
+    cmax(sizeof(WarpDiag) * kWarps,
+         cmax(sizeof(RowsSm), kOpsOffset + umma::kSmemFloats * sizeof(float)));
 
 // Exclusive prefix of cnt(i) over i in [0, nl) into P.ptr (CTA-wide; nl <=
 // kChunkFronts). Returns the total.
@@ -740,9 +746,10 @@ __device__ void phase_a_item(const DevState& s, const FactorParams& prm, BigFron
 
 // ---------------------------------------------------------------- phase U
 
-// One 64 x 64 lower tile (I, J) of front B's trailing matrix, rank-kw update
-// with the panel's L (columns kstart..kstart+kw of F) and W (Wg).
-__device__ void phase_u_tile(const DevState& s, const BigFront& B, int I, int J, UpdSm& sm) {
+// One 64 x 64 lower tile of front B's trailing matrix at rows i0, columns
+// j0: the rank-kw update with the panel's L (columns kstart..kstart+kw of F)
+// and W (Wg), in FP64.
+__device__ void phase_u_tile(const DevState& s, const BigFront& B, int i0, int j0, UpdSm& sm) {
   const int tid = threadIdx.x;
   const int tx = tid & 15;
   const int ty = tid >> 4;
@@ -752,8 +759,6 @@ __device__ void phase_u_tile(const DevState& s, const BigFront& B, int I, int J,
   const int ks = B.kstart;
   double* F = s.dpool + B.doff;
   const double* W = s.dpool + B.woff;
-  const int i0 = k + I * kTileU;
-  const int j0 = k + J * kTileU;
   double cur[4][4];
 #pragma unroll
   for (int b = 0; b < 4; b++) {
@@ -817,7 +822,7 @@ __device__ void phase_u_tile(const DevState& s, const BigFront& B, int I, int J,
       if (i < f && i >= j) F[i + (size_t)f * j] = cur[a][b] - acc[a][b];
     }
   }
-  if (J == 0) {
+  if (j0 == k) {
     // the next panel's columns [k, k + 32): their largest magnitude over the
     // rows below the next block, for its first test (the 16 threads with
     // the same ty are one half-warp)
@@ -841,9 +846,43 @@ __device__ void phase_u_tile(const DevState& s, const BigFront& B, int I, int J,
   __syncthreads();
 }
 
-__device__ __forceinline__ long long tri_tiles(const BigFront& B) {
-  const long long t = (B.f - B.k + kTileU - 1) / kTileU;
+__device__ __forceinline__ long long tri_tiles(const BigFront& B, int tile) {
+  const long long t = (B.f - B.k + tile - 1) / tile;
   return t * (t + 1) / 2;
+}
+
+__device__ __forceinline__ void tri_decode(long long lt, int& I, int& J) {
+  I = (int)((sqrt(8.0 * (double)lt + 1.0) - 1.0) * 0.5);
+  while ((long long)(I + 1) * (I + 2) / 2 <= lt) I++;
+  while ((long long)I * (I + 1) / 2 > lt) I--;
+  J = (int)(lt - (long long)I * (I + 1) / 2);
+}
+
+// Mixed precision: a 128 x 128 tile (I, J) of the trailing matrix. Tiles of
+// the contribution block (columns from fs on: rows that the parent
+// assembles, never pivoted in this front) take the update on the tensor
+// cores (umma.cuh, 3xTF32 products accumulated in FP32); the others, which
+// hold the fully summed columns whose pivots are still to be decided, stay
+// in FP64 as four 64 x 64 tiles. Returns 1 if a tensor-core operation did
+// not complete in time.
+__device__ int phase_u_tile_mixed(const DevState& s, const BigFront& B, int I, int J, UpdSm& sm,
+                                  float* ops, uint64_t* mbar, uint32_t* phase, uint32_t tmem) {
+  const int f = B.f, k = B.k;
+  const int i0 = k + I * umma::kTileM;
+  const int j0 = k + J * umma::kTileN;
+  if (j0 >= B.fs) {
+    double* F = s.dpool + B.doff;
+    const double* W = s.dpool + B.woff;
+    return umma::tile_update(F, f, F + (size_t)f * B.kstart, f, W, f, i0, j0,
+                             min(umma::kTileM, f - i0), min(umma::kTileN, f - j0), B.kw, I == J,
+                             ops, mbar, phase, tmem);
+  }
+  for (int a = 0; a < 2; a++)
+    for (int b = 0; b < 2; b++) {
+      const int si = i0 + a * kTileU, sj = j0 + b * kTileU;
+      if (si < f && sj < f && si + kTileU - 1 >= sj) phase_u_tile(s, B, si, sj, sm);
+    }
+  return 0;
 }
 
 // ---------------------------------------------------------------- the level
@@ -852,12 +891,25 @@ __global__ void __launch_bounds__(kThreads, 1)
     app_level_kernel(DevState s, FactorParams prm, const int* __restrict__ list, int nl,
                      int max_steps, int* counters) {
   cg::grid_group grid = cg::this_grid();
-  extern __shared__ __align__(16) unsigned char dsm[];
+  extern __shared__ __align__(1024) unsigned char dsm[];
   __shared__ Prefix P;
+  __shared__ __align__(8) uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
   const int gwarp = blockIdx.x * kWarps + warp;
   const int nwarp = gridDim.x * kWarps;
+  // mixed precision: 128 tensor-memory columns per CTA for the accumulator
+  uint32_t tmem = 0, phase = 0;
+  int tc_fail = 0;
+  if (prm.mixed) {
+    if (warp == 0) umma::tmem_alloc_128(&tmem_slot);
+    if (tid == 0) umma::mbar_init(&mbar);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::);
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::);
+    tmem = tmem_slot;
+  }
   int step = 1;
   for (; step <= max_steps; step++) {
     // ---- D: one warp per front
@@ -900,22 +952,27 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     grid.sync();
     // ---- U: trailing-update tiles of the fronts that accepted pivots
+    const int tile = prm.mixed ? umma::kTileM : kTileU;
     for (int c0 = 0; c0 < nl; c0 += kChunkFronts) {
       const int n = min(kChunkFronts, nl - c0);
       const long long total = front_prefix(P, n, [&](int i) {
         const BigFront& B = s.big[list[c0 + i]];
-        return (active(s, B, step) && B.kw > 0) ? tri_tiles(B) : 0ll;
+        return (active(s, B, step) && B.kw > 0) ? tri_tiles(B, tile) : 0ll;
       });
       UpdSm& sm = *reinterpret_cast<UpdSm*>(dsm);
       for (long long t = blockIdx.x; t < total; t += gridDim.x) {
         const int fi = item_front(P, n, t);
         const BigFront& B = s.big[list[c0 + fi]];
-        const long long lt = t - P.ptr[fi];
-        int I = (int)((sqrt(8.0 * (double)lt + 1.0) - 1.0) * 0.5);
-        while ((long long)(I + 1) * (I + 2) / 2 <= lt) I++;
-        while ((long long)I * (I + 1) / 2 > lt) I--;
-        const int J = (int)(lt - (long long)I * (I + 1) / 2);
-        phase_u_tile(s, B, I, J, sm);
+        int I, J;
+        tri_decode(t - P.ptr[fi], I, J);
+        if (!prm.mixed) {
+          phase_u_tile(s, B, B.k + I * kTileU, B.k + J * kTileU, sm);
+        } else if (!tc_fail) {
+          // the tensor-core operands share the dynamic shared memory with
+          // the FP64 tiles' panels (a tile uses one or the other)
+          float* ops = reinterpret_cast<float*>(dsm + kOpsOffset);
+          tc_fail = phase_u_tile_mixed(s, B, I, J, sm, ops, &mbar, &phase, tmem);
+        }
       }
       __syncthreads();
     }
@@ -923,6 +980,17 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   // the step cap (never reached when every step makes progress)
   if (step > max_steps && blockIdx.x == 0 && tid == 0) counters[2] = 1;
+  if (prm.mixed) {
+    if (tc_fail) {
+      // a tensor-core operation did not complete in time: the factorization
+      // is reported failed; wait once more (bounded) before freeing TMEM
+      if (tid == 0) counters[2] = 2;
+      umma::mbar_wait(&mbar, phase ^ 1u);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::);
+    __syncthreads();
+    if (warp == 0) umma::tmem_free_128(tmem);
+  }
 }
 
 }  // namespace

@@ -176,6 +176,9 @@ struct FactorParams {
   // of app_min_f rows up
   int app;
   int app_min_f;
+  // mixed precision: the contribution-block tiles of the a-posteriori panels'
+  // trailing updates on the tensor cores (3xTF32, FP32 accumulation)
+  int mixed;
 };
 
 // Largest front factored entirely in shared memory (fp64, ld = f | 1).

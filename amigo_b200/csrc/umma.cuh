@@ -143,7 +143,7 @@ __device__ __forceinline__ int op_index(int m, int k) {
 // whole CTA calls it (blockDim.x = 128 or 256). ops: kSmemFloats floats of
 // shared memory aligned to 128 bytes. *phase tracks the mbarrier's parity.
 // Returns 0, or 1 if an MMA did not complete within the spin bound.
-__device__ int tile_update(double* C, long long ldc, const double* A, long long lda,
+__device__ __noinline__ static int tile_update(double* C, long long ldc, const double* A, long long lda,
                            const double* B, long long ldb, long long i0, long long j0, int mrows,
                            int ncols, int kk, bool lower_only, float* ops, uint64_t* mbar,
                            uint32_t* phase, uint32_t tmem) {

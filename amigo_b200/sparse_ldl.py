@@ -394,6 +394,32 @@ class SparseLDL:
         _native.check(self._h, st, "node_pivots")
         return a, b
 
+    # -- precision -------------------------------------------------------------------
+    def set_precision(self, mode: str = "fp64", refine_iters: int = 5, refine_tol: float = 1e-12):
+        """``"fp64"`` (the default) or ``"mixed"``: after pivot-order reuse, the
+        contribution-block tiles of the big fronts' trailing updates run on
+        the tensor cores with about FP32 accuracy, and every solve is refined
+        in FP64 against the factored matrix (at most ``refine_iters``
+        corrections, until the backward error is <= ``refine_tol``)."""
+        code = {"fp64": 0, "mixed": 1}[mode]
+        _native.check(self._h, self._lib.b200ldl_set_precision(self._h, code), "set_precision")
+        _native.check(self._h, self._lib.b200ldl_set_refinement(self._h, int(refine_iters),
+                                                                float(refine_tol)),
+                      "set_refinement")
+
+    def last_refinement(self) -> dict:
+        """Corrections and largest backward error of the last refined solve,
+        whether the factor in use ran mixed-precision tiles, and how many
+        factorizations the mixed-precision checks redid in FP64."""
+        it = ctypes.c_int()
+        be = ctypes.c_double()
+        mx = ctypes.c_int()
+        fb = ctypes.c_int()
+        self._lib.b200ldl_last_refinement(self._h, ctypes.byref(it), ctypes.byref(be),
+                                          ctypes.byref(mx), ctypes.byref(fb))
+        return {"iterations": it.value, "backward_error": be.value, "mixed": bool(mx.value),
+                "fp64_redos": fb.value}
+
     # -- pivot-order reuse --------------------------------------------------------
     def pivot_record(self) -> dict:
         """The last factorization's pivot record: per supernode the front size

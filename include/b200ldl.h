@@ -96,6 +96,39 @@ int b200ldl_solve_refine(b200ldl_t h, const double* vals, const double* diag,
                          int ldx, int max_iter, double tol, double* berr_out,
                          int* iters_out);
 
+/* Precision of the factorization (no counterpart in the reference, which
+ * computes everything in FP64, include/sparse_ldl.h:1190-1215 and
+ * 1316-1553). B200LDL_FP64 (the default): every update in FP64.
+ * B200LDL_MIXED: in the blocked panels that fronts re-planned from a pivot
+ * record use (b200ldl_set_pivot_record), the trailing-update tiles of the
+ * contribution block (the rows the parent assembles, never pivoted in the
+ * front) run on the tensor cores with about FP32 accuracy (see
+ * b200ldl_schur_update_tc); the fully summed columns, every pivot decision
+ * and all other fronts stay in FP64. Two checks keep the results those of
+ * an FP64 factorization: a mixed factorization whose inertia differs from
+ * the last FP64 factorization of the handle is redone in FP64 (FP32-level
+ * rounding can flip the sign of a pivot that cancellation makes tiny; with
+ * no FP64 factorization on the handle yet the factorization runs in FP64),
+ * and b200ldl_solve / b200ldl_solve_host refine every solution in FP64
+ * against the factored matrix (the vals and diag of the factor call, which
+ * must stay valid until the solves) to the tolerance of
+ * b200ldl_set_refinement, refactoring in FP64 and solving again if the
+ * refinement stalls. Applies from the next factorization. */
+#define B200LDL_FP64 0
+#define B200LDL_MIXED 1
+int b200ldl_set_precision(b200ldl_t h, int mode);
+
+/* Refinement of the solves after a mixed-precision factorization: at most
+ * max_iter corrections per solve, until every column's backward error is
+ * <= tol (defaults 5 and 1e-12). */
+int b200ldl_set_refinement(b200ldl_t h, int max_iter, double tol);
+
+/* The last refinement: corrections used, the largest backward error,
+ * whether the factor in use ran mixed tiles, and how many factorizations of
+ * the handle the mixed-precision checks redid in FP64 (any pointer may be
+ * NULL). */
+int b200ldl_last_refinement(b200ldl_t h, int* iters, double* berr, int* mixed, int* fallbacks);
+
 /* Inertia of the last factorization: numbers of positive and negative
  * pivots (zero pivots count as positive, as the reference does). Replaces
  * SparseLDL::get_inertia (include/sparse_ldl.h:205-213). */
