@@ -418,6 +418,32 @@ def run_ours(args, world, rank, local):
         ldl.set_profiling(False)
     value = world * args.steps / (ms_max / 1e3)
 
+    # (4) mixed precision on the same pivot order: contribution-block tiles on
+    # the tensor cores, FP64-refined solves, FP64 redo when the inertia
+    # differs from the FP64 factorization's or the refinement stalls
+    mixed = None
+    if not args.no_mixed:
+        ldl.set_precision("mixed", refine_iters=5, refine_tol=BERR_TARGET)
+        for _ in range(args.warmup):
+            step()
+        redo0 = ldl.last_refinement()["fp64_redos"]
+        ms_mixed = timed(args.steps)
+        info = ldl.last_refinement()
+        berr_mixed = backward_error(s, x.cpu().numpy(), s.rhs)
+        mixed = {
+            "value": world * args.steps / (ms_mixed / 1e3),
+            "ms_per_step": ms_mixed / args.steps, "backward_error": berr_mixed,
+            "berr_target_met": bool(berr_mixed <= BERR_TARGET),
+            "inertia": list(ldl.get_inertia()),
+            "fp64_redos_in_timed_steps": info["fp64_redos"] - redo0,
+            "refinement_iterations": info["iterations"],
+            "vs_fp64_same_pivot_order": (ms_max / args.steps) / (ms_mixed / args.steps),
+            "what": "contribution-block tiles of the big fronts' trailing updates as 3xTF32 on "
+                    "tcgen05 (FP32 accumulation in tensor memory), solves refined in FP64 to "
+                    "1e-10; a factorization whose inertia differs from the FP64 one is redone "
+                    "in FP64 (on this KKT family FP32-level rounding flips tiny pivots)"}
+        ldl.set_precision("fp64")
+
     # end to end through the public API with host buffers (pinned), the same
     # reuse of the previous factorization's pivot order (the device-buffer
     # handle is released first: each holds the factor pools of this system)
@@ -551,7 +577,7 @@ def run_ours(args, world, rank, local):
             "inertia": list(inertia_iterate), "delayed_pivots": delayed_iterate,
             "what": "record taken from values perturbed by 1% (entries) and exp(0.3 N(0,1)) "
                     "(Sigma), then the benchmark matrix factored with it"},
-        "mixed_precision": None,
+        "mixed_precision": mixed,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "backward_error": berr_e2e},
         "roofline": roof,
@@ -698,6 +724,7 @@ def main(argv=None) -> int:
     ap.add_argument("--no-e2e", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-profile-pass", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-clocks", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--no-mixed", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--workload", choices=["plane_stress", "batched"], default="plane_stress",
                     help=argparse.SUPPRESS)
     ap.add_argument("--systems", type=int, default=512, help=argparse.SUPPRESS)

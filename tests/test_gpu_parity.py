@@ -92,6 +92,17 @@ def test_plane_stress_delayed_pivots(nel):
     assert abs(int(ndel_g.sum()) - int(ndel_r.sum())) <= max(8, 0.02 * ndel_r.sum())
 
 
+def test_plane_stress_256_benchmark_system():
+    """The benchmark's system itself (256 x 256, n = 329,732): inertia equal
+    to the compiled reference's and the designed one, FP64 backward error,
+    forward agreement with the reference's FP64 solve, and the delayed-pivot
+    totals of the reference's pivot sequence."""
+    g, r = _check_system(plane_stress_kkt(256))
+    npiv_g, ndel_g = g.node_pivots()
+    npiv_r, ndel_r = r.node_pivots()
+    assert abs(int(ndel_g.sum()) - int(ndel_r.sum())) <= max(8, 0.02 * ndel_r.sum())
+
+
 def test_torch_device_path():
     torch = pytest.importorskip("torch")
     s = optimal_control_kkt(N=300)
