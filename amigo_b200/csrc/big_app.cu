@@ -99,9 +99,6 @@ __device__ __forceinline__ double fsym(const double* F, int f, int a, int b) {
 }
 
 __device__ __forceinline__ int* xint(double* X) { return reinterpret_cast<int*>(X + kXInt); }
-__device__ __forceinline__ const int* xint(const double* X) {
-  return reinterpret_cast<const int*>(X + kXInt);
-}
 
 // largest value, lowest index on ties (idamax)
 __device__ __forceinline__ void warp_argmax(double& v, int& i) {
@@ -122,35 +119,6 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-// The reference's tests for the accepted pivots of a panel, with the column
-// maxima over the whole front: number of leading pivots that pass.
-__device__ int passing_prefix(const double* X, double ustab, double tol) {
-  const int* xi = xint(X);
-  const int acc = xi[kIAcc];
-  const unsigned long long* below = reinterpret_cast<const unsigned long long*>(X + kXBelow);
-  int p = 0;
-  while (p < acc) {
-    const int kind = xi[kIKind + p];
-    const double cb = __longlong_as_double((long long)below[p]);
-    if (kind == 1) {
-      const double d = X[kXD + 3 * p];
-      const double cm = fmax(X[kXCin + p], cb);
-      if (!(fabs(d) >= tol && fabs(d) >= ustab * cm)) break;
-      p += 1;
-    } else {
-      const double d11 = X[kXD + 3 * p], d21 = X[kXD + 3 * p + 1], d22 = X[kXD + 3 * p + 2];
-      const double det = fabs(d11 * d22 - d21 * d21);
-      const double ad21 = fabs(d21);
-      const double delta = det / fmax(fabs(d22) + ad21, fabs(d11) + ad21);
-      const double cm = fmax(X[kXCin + p], cb);
-      const double rm = fmax(X[kXRin + p], __longlong_as_double((long long)below[p + 1]));
-      if (!(det >= tol && delta >= ustab * cm && delta >= ustab * rm)) break;
-      p += 2;
-    }
-  }
-  return p;
-}
-
 // ------------------------------------------------------------- shared memory
 
 struct WarpDiag {  // phase D, one per warp
@@ -158,15 +126,43 @@ struct WarpDiag {  // phase D, one per warp
   double Lb[kBlk][kLd];
   double dd[3 * kBlk], cin[kBlk], rin[kBlk], below0[kBlk];
   int perm[kBlk], kind[kBlk], dlt[kBlk];
+  int var[kBlk], part[kBlk];  // block candidates' variables and recorded 2x2 partners
 };
 
 struct RowsSm {  // phases R and A
   double Ls[kBlk][kLd];
   double red[kWarps][kBlk];
   double sd[3 * kBlk], sinv[kBlk];
+  double scm[kBlk], srm[kBlk];  // phase A: column maxima over the front, 2x2 partner's block part
   int sperm[kBlk], skind[kBlk];
   int np;
 };
+
+// The reference's tests for the accepted pivots of a panel, with the column
+// maxima over the whole front (staged in shared memory by phase A): number
+// of leading pivots that pass.
+__device__ int passing_prefix(const RowsSm& sm, int acc, double ustab, double tol) {
+  int p = 0;
+  while (p < acc) {
+    const double cm = sm.scm[p];
+    if (sm.skind[p] == 1) {
+      const double d = sm.sd[3 * p];
+      if (!(fabs(d) >= tol && fabs(d) >= ustab * cm)) break;
+      p += 1;
+    } else {
+      const double d11 = sm.sd[3 * p], d21 = sm.sd[3 * p + 1], d22 = sm.sd[3 * p + 2];
+      const double det = fabs(d11 * d22 - d21 * d21);
+      const double ad21 = fabs(d21);
+      const double delta = det / fmax(fabs(d22) + ad21, fabs(d11) + ad21);
+      // the partner's maximum: its block part (srm) and its maximum below
+      // (scm of the second position, whose block part phase D leaves at 0)
+      const double rm = fmax(sm.srm[p], sm.scm[p + 1]);
+      if (!(det >= tol && delta >= ustab * cm && delta >= ustab * rm)) break;
+      p += 2;
+    }
+  }
+  return p;
+}
 
 struct UpdSm {  // phase U
   double As[kBigPanelMax][kTileU];
@@ -323,10 +319,27 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
   const int k = B->k;
   const int ncand = B->ncand;
   const int nbk = max(0, min(kBlk, ncand - k));
-  for (int t = lane; t < kBlk * kBlk; t += 32) {
-    const int i = t % kBlk, j = t / kBlk;
-    w.A[i][j] = (i < nbk && j < nbk) ? fsym(F, f, k + i, k + j) : 0.0;
-    w.Lb[i][j] = 0.0;
+  {
+    // the block's lower triangle, one coalesced column per load (all loads
+    // in flight before the shared-memory stores), mirrored above
+    double v[kBlk];
+#pragma unroll
+    for (int j = 0; j < kBlk; j++)
+      v[j] = (j <= lane && lane < nbk) ? F[(k + lane) + (size_t)f * (k + j)] : 0.0;
+    // the candidates' variables and the partners they had in the record
+    const int var = (lane < nbk) ? fv[k + lane] : -1;
+    const int part = (var >= 0 && s.partner) ? s.partner[var] : -1;
+    // entry (i, j) and its mirror are written by lane max(i, j) only
+#pragma unroll
+    for (int j = 0; j < kBlk; j++) {
+      if (j <= lane) {
+        w.A[lane][j] = v[j];
+        w.A[j][lane] = v[j];
+      }
+      w.Lb[lane][j] = 0.0;
+    }
+    w.var[lane] = var;
+    w.part[lane] = part;
   }
   w.perm[lane] = lane;
   w.kind[lane] = 0;
@@ -367,9 +380,9 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
     // rows would accept the first of them alone and the a-posteriori test
     // would then reject it
     bool hinted = false;
-    if (has && s.partner) {
-      const int vt = fv[k + w.perm[t]], vn = fv[k + w.perm[t + 1]];
-      hinted = vt >= 0 && vn >= 0 && s.partner[vt] == vn;
+    if (has) {
+      const int pt = w.perm[t], vn = w.var[w.perm[t + 1]];
+      hinted = w.var[pt] >= 0 && vn >= 0 && w.part[pt] == vn;
     }
     if (hinted) {
       const double r2 =
@@ -637,7 +650,6 @@ __device__ void phase_a_item(const DevState& s, const FactorParams& prm, BigFron
   const int f = B->f;
   const int k = xi[kIK];
   const int nbk = xi[kINbk];
-  if (tid == 0) sm.np = passing_prefix(X, prm.ustab, prm.pivot_tol);
   for (int t = tid; t < kBlk * kLd; t += kThreads) (&sm.Ls[0][0])[t] = X[kXL + t];
   if (tid < kBlk) {
     sm.skind[tid] = xi[kIKind + tid];
@@ -646,7 +658,12 @@ __device__ void phase_a_item(const DevState& s, const FactorParams& prm, BigFron
     sm.sd[3 * tid + 2] = X[kXD + 3 * tid + 2];
     // 1x1 pivots scale their column by 1/d, as the reference does
     sm.sinv[tid] = (xi[kIKind + tid] == 1) ? 1.0 / X[kXD + 3 * tid] : 0.0;
+    const unsigned long long* below = reinterpret_cast<const unsigned long long*>(X + kXBelow);
+    sm.scm[tid] = fmax(X[kXCin + tid], __longlong_as_double((long long)below[tid]));
+    sm.srm[tid] = X[kXRin + tid];
   }
+  __syncthreads();
+  if (tid == 0) sm.np = passing_prefix(sm, xi[kIAcc], prm.ustab, prm.pivot_tol);
   __syncthreads();
   const int np = sm.np;
   double* F = s.dpool + B->doff;
