@@ -114,7 +114,6 @@ struct b200ldl_handle {
   std::vector<int64_t> hp_scat_ptr;
   int num_levels = 0;
   std::vector<int> level_ptr;  // host copy
-  std::vector<int> level_maxkids;
   // a level whose fronts cannot exceed the shared-memory limit, whatever the
   // delays, needs no big-front launch (and no host read-back)
   std::vector<char> level_may_big;
@@ -289,12 +288,6 @@ void build_plan(b200ldl_t h, const int* rowp, const int* cols) {
     for (int k = 0; k < nn; k++)
       if (fsb[k] + nc[k] > kSmemFrontMax) h->level_may_big[level[k]] = 1;
   }
-  h->level_maxkids.assign(nl, 0);
-  for (int l = 0; l < nl; l++)
-    for (int q = lptr[l]; q < lptr[l + 1]; q++) {
-      const int k = lnodes[q];
-      h->level_maxkids[l] = std::max(h->level_maxkids[l], kid_ptr[k + 1] - kid_ptr[k]);
-    }
   h->h_ns = ns;
   h->h_nc = nc;
   h->hp_ns = std::move(ns);
@@ -570,7 +563,7 @@ void run_factor_once(b200ldl_t h, const double* vals, const double* diag, bool m
           info.class_maxf[c] = meta[10 + c];
           if (meta[5 + c] > 0) info.cluster_launches++;
         }
-        CK(launch_big_level(h->plan, h->st, info, h->level_maxkids[l], prm, vals, diag,
+        CK(launch_big_level(h->plan, h->st, info, prm, vals, diag,
                             h->stream, h->prof));
       }
     }

@@ -88,105 +88,110 @@ __device__ void block_reduce(BlockRed& r, double& bv, int& bi, double& cm) {
 
 // ---------------------------------------------------------------- assembly
 
-__global__ void big_zero_kernel(DevState s, const int* __restrict__ list) {
-  const BigFront& B = s.big[list[blockIdx.x]];
-  double* F = s.dpool + B.doff;
-  const int f = B.f;
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int nw = blockDim.x >> 5;
-  for (int j = blockIdx.y * nw + warp; j < f; j += gridDim.y * nw) {
-    double* col = F + (size_t)f * j;
-    for (int i = j + lane; i < f; i += 32) col[i] = 0.0;
-  }
-  // a-posteriori panels: no column maxima for the first panel yet
-  if (B.app && blockIdx.y == 0 && threadIdx.x < kBigPanelMax)
-    s.dpool[B.xoff + kAppNextColmax + threadIdx.x] = 0.0;
+// Assembly of every big front of a level in one launch: a front per
+// cluster of CL CTAs (CL = 1: a front per CTA). The cluster zeroes the
+// front's lower triangle with Sigma already on the own variables' diagonal,
+// adds the CSR entries of its pivot columns, then extend-adds its children's
+// contribution blocks one child after another, with a cluster barrier
+// between the steps. Each entry therefore receives its terms in the order
+// diag, CSR value, children in child order; since the front starts at zero
+// and each position receives at most one CSR value, d + v is the same
+// number as the (0 + v) + d of adding the diagonal after the values, as
+// SparseLDL::assemble_front_matrix followed by factor's add_diagonal does
+// (include/sparse_ldl.h:1078-1104).
+template <int CL>
+__device__ __forceinline__ void asm_sync() {
+  if constexpr (CL == 1)
+    __syncthreads();
+  else
+    cg::this_cluster().sync();
 }
 
-__global__ void big_scatter_kernel(DevPlan p, DevState s, const double* __restrict__ vals,
-                                   const double* __restrict__ diag,
-                                   const int* __restrict__ list) {
-  const BigFront& B = s.big[list[blockIdx.x]];
+template <int CL>
+__global__ void __launch_bounds__(256) big_assemble_kernel(DevPlan p, DevState s,
+                                                          const double* __restrict__ vals,
+                                                          const double* __restrict__ diag,
+                                                          const int* __restrict__ list) {
+  const BigFront& B = s.big[list[blockIdx.x / CL]];
+  const int rank = (int)(blockIdx.x % CL);
   double* F = s.dpool + B.doff;
   const int f = B.f, ns = B.ns, nd_in = B.nd_in, node = B.node;
-  const int64_t e0 = p.scat_ptr[node];
-  const int64_t e1 = p.scat_ptr[node + 1];
-  const int64_t stride = (int64_t)gridDim.y * blockDim.x;
-  for (int64_t e = e0 + (int64_t)blockIdx.y * blockDim.x + threadIdx.x; e < e1; e += stride) {
-    int r = p.scat_row[e];
-    if (r >= ns) r += nd_in;
-    F[r + (size_t)f * p.scat_col[e]] += vals[p.scat_csr[e]];
-  }
-}
-
-__global__ void big_diag_kernel(DevPlan p, DevState s, const double* __restrict__ diag,
-                                const int* __restrict__ list) {
-  const BigFront& B = s.big[list[blockIdx.x]];
-  double* F = s.dpool + B.doff;
-  const int f = B.f;
-  const int v0 = p.var_ptr[B.node];
-  for (int j = threadIdx.x; j < B.ns; j += blockDim.x)
-    F[j + (size_t)f * j] += diag[p.node_to_var[v0 + j]];
-}
-
-// extend-add of the c-th child of every big front
-__global__ void big_extend_kernel(DevPlan p, DevState s, int c, const int* __restrict__ list) {
-  const BigFront& B = s.big[list[blockIdx.x]];
-  const int node = B.node;
-  const int kb = p.kid_ptr[node];
-  const int ke = p.kid_ptr[node + 1];
-  if (kb + c >= ke) return;
-  double* F = s.dpool + B.doff;
-  const int f = B.f, ns = B.ns, nd_in = B.nd_in;
-  int off = ns;
-  for (int q = kb; q < kb + c; q++) off += s.ndel[p.kids[q]];
-  const int ch = p.kids[kb + c];
-  const int nd = s.ndel[ch];
-  const int m = s.f[ch] - s.npiv[ch];
-  const double* cb = s.dpool + s.cb_off[ch];
-  const int cld = s.cb_ld[ch];
-  const int* cm = p.cmap + p.cptr[ch];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const int nw = blockDim.x >> 5;
-  for (int r2 = blockIdx.y * nw + warp; r2 < m; r2 += gridDim.y * nw) {
-    int p2;
-    if (r2 < nd) {
-      p2 = off + r2;
-    } else {
-      p2 = cm[r2 - nd];
-      if (p2 >= ns) p2 += nd_in;
+  constexpr int kW = 8;  // warps per CTA
+  const int v0 = p.var_ptr[node];
+  // zero, with the diagonal of the own variables set to Sigma
+  for (int j = rank * kW + warp; j < f; j += CL * kW) {
+    double* col = F + (size_t)f * j;
+    const double dj = (diag && j < ns) ? diag[p.node_to_var[v0 + j]] : 0.0;
+    for (int i = j + lane; i < f; i += 32) col[i] = (i == j) ? dj : 0.0;
+  }
+  // a-posteriori panels: no column maxima for the first panel yet
+  if (B.app && rank == 0 && threadIdx.x < kBigPanelMax)
+    s.dpool[B.xoff + kAppNextColmax + threadIdx.x] = 0.0;
+  asm_sync<CL>();
+  // the CSR entries of the pivot columns (distinct positions)
+  {
+    const int64_t e0 = p.scat_ptr[node];
+    const int64_t e1 = p.scat_ptr[node + 1];
+    for (int64_t e = e0 + (int64_t)rank * blockDim.x + threadIdx.x; e < e1;
+         e += (int64_t)CL * blockDim.x) {
+      int r = p.scat_row[e];
+      if (r >= ns) r += nd_in;
+      F[r + (size_t)f * p.scat_col[e]] += vals[p.scat_csr[e]];
     }
-    const double* col = cb + (size_t)cld * r2;
-    // four entries per lane pass: their loads (map, value, front) are in
-    // flight together before the read-modify-writes
-    for (int rb = r2 + lane; rb < m; rb += 128) {
-      double* dst[4];
-      double val[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const int r1 = rb + 32 * u;
-        dst[u] = nullptr;
-        if (r1 < m) {
-          int p1;
-          if (r1 < nd) {
-            p1 = off + r1;
-          } else {
-            p1 = cm[r1 - nd];
-            if (p1 >= ns) p1 += nd_in;
-          }
-          dst[u] = (p1 >= p2) ? F + (p1 + (size_t)f * p2) : F + (p2 + (size_t)f * p1);
-          val[u] = col[r1];
-        }
+  }
+  // the children's contribution blocks, one child after another
+  const int kb = p.kid_ptr[node];
+  const int ke = p.kid_ptr[node + 1];
+  int off = ns;  // first position of this child's delayed rows
+  for (int q = kb; q < ke; q++) {
+    asm_sync<CL>();
+    const int ch = p.kids[q];
+    const int nd = s.ndel[ch];
+    const int m = s.f[ch] - s.npiv[ch];
+    const double* cb = s.dpool + s.cb_off[ch];
+    const int cld = s.cb_ld[ch];
+    const int* cm = p.cmap + p.cptr[ch];
+    for (int r2 = rank * kW + warp; r2 < m; r2 += CL * kW) {
+      int p2;
+      if (r2 < nd) {
+        p2 = off + r2;
+      } else {
+        p2 = cm[r2 - nd];
+        if (p2 >= ns) p2 += nd_in;
       }
-      double old[4];
+      const double* col = cb + (size_t)cld * r2;
+      // four entries per lane pass: their loads (map, value, front) are in
+      // flight together before the read-modify-writes
+      for (int rb = r2 + lane; rb < m; rb += 128) {
+        double* dst[4];
+        double val[4];
 #pragma unroll
-      for (int u = 0; u < 4; u++) old[u] = dst[u] ? *dst[u] : 0.0;
+        for (int u = 0; u < 4; u++) {
+          const int r1 = rb + 32 * u;
+          dst[u] = nullptr;
+          if (r1 < m) {
+            int p1;
+            if (r1 < nd) {
+              p1 = off + r1;
+            } else {
+              p1 = cm[r1 - nd];
+              if (p1 >= ns) p1 += nd_in;
+            }
+            dst[u] = (p1 >= p2) ? F + (p1 + (size_t)f * p2) : F + (p2 + (size_t)f * p1);
+            val[u] = col[r1];
+          }
+        }
+        double old[4];
 #pragma unroll
-      for (int u = 0; u < 4; u++)
-        if (dst[u]) *dst[u] = old[u] + val[u];
+        for (int u = 0; u < 4; u++) old[u] = dst[u] ? *dst[u] : 0.0;
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (dst[u]) *dst[u] = old[u] + val[u];
+      }
     }
+    off += nd;
   }
 }
 
@@ -784,31 +789,52 @@ cudaError_t launch_panel(const DevState& s, const FactorParams& prm, int count, 
 
 constexpr size_t kPanelSmemMax = 224 * 1024;
 
-void assemble_big(const DevPlan& p, const DevState& s, const int* list, int nl, int max_f,
-                  int maxkids, const double* vals, const double* diag, cudaStream_t stream,
-                  Prof& prof) {
-  const int ych = std::min(256, (max_f + 7) / 8);
-  prof.begin(stream);
-  big_zero_kernel<<<dim3(nl, ych), 256, 0, stream>>>(s, list);
-  big_scatter_kernel<<<dim3(nl, 16), 256, 0, stream>>>(p, s, vals, diag, list);
-  if (diag) big_diag_kernel<<<nl, 256, 0, stream>>>(p, s, diag, list);
-  for (int c = 0; c < maxkids; c++)
-    big_extend_kernel<<<dim3(nl, ych), 256, 0, stream>>>(p, s, c, list);
-  prof.end(kPhBigAsm, stream, 2 + (diag ? 1 : 0) + maxkids);
+template <int CL>
+cudaError_t launch_assemble_cl(const DevPlan& p, const DevState& s, const int* list, int nl,
+                               const double* vals, const double* diag, cudaStream_t stream) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(nl * CL), 1, 1);
+  cfg.blockDim = dim3(256, 1, 1);
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = CL > 1 ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, big_assemble_kernel<CL>, p, s, vals, diag, list);
 }
 
+// One launch for the level's fronts in `list`: a CTA per front when they
+// fill the GPU, otherwise a cluster of 4 or 16 CTAs per front.
+cudaError_t assemble_big(const DevPlan& p, const DevState& s, const int* list, int nl,
+                         const double* vals, const double* diag, cudaStream_t stream,
+                         Prof& prof) {
+  if (nl <= 0) return cudaSuccess;
+  prof.begin(stream);
+  cudaError_t e;
+  if (nl >= 148)
+    e = launch_assemble_cl<1>(p, s, list, nl, vals, diag, stream);
+  else if (nl >= 37)
+    e = launch_assemble_cl<4>(p, s, list, nl, vals, diag, stream);
+  else
+    e = launch_assemble_cl<16>(p, s, list, nl, vals, diag, stream);
+  prof.end(kPhBigAsm, stream, 1);
+  return e;
+}
 
 // Class-6 fronts: blocked panels with a-posteriori tests (big_app.cu), all
 // of the level's panel steps in one cooperative launch.
 cudaError_t app_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
-                      int maxkids, const FactorParams& prm, const double* vals,
+                      const FactorParams& prm, const double* vals,
                       const double* diag, cudaStream_t stream, Prof& prof) {
   const int nl = info.count_app;
   const int* list6 = s.class_list + (size_t)6 * p.num_nodes;
-  assemble_big(p, s, list6, nl, info.max_f_app, maxkids, vals, diag, stream, prof);
+  cudaError_t e = assemble_big(p, s, list6, nl, vals, diag, stream, prof);
+  if (e != cudaSuccess) return e;
   prof.begin(stream);
-  cudaError_t e =
-      launch_app_level(s, prm, nl, info.max_fs_app, list6, s.big_meta + 21, stream);
+  e = launch_app_level(s, prm, nl, info.max_fs_app, list6, s.big_meta + 21, stream);
   if (e != cudaSuccess) return e;
   prof.end(kPhBigPanel, stream, 1);
   int cap = 0;
@@ -832,18 +858,19 @@ cudaError_t configure_big_kernels() {
   e = cudaFuncSetAttribute(big_panel_kernel<16>,
                            cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(big_assemble_kernel<16>,
+                           cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e != cudaSuccess) return e;
   e = configure_big_chain_kernel();
   if (e != cudaSuccess) return e;
   return configure_cluster_front_kernels();
 }
 
 cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
-                             int maxkids, const FactorParams& prm, const double* vals,
+                             const FactorParams& prm, const double* vals,
                              const double* diag, cudaStream_t stream, Prof& prof) {
   const int nb = info.count;
   if (nb <= 0) return cudaSuccess;
-  const int cols_per = 8;  // warps per CTA in the assembly kernels
-  const int ychunks = std::min(256, (info.max_f + cols_per - 1) / cols_per);
   prof.begin(stream);
 
   // fronts that fit in a cluster's distributed shared memory
@@ -854,7 +881,7 @@ cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevel
   }
   prof.end(kPhCluster, stream, info.cluster_launches);
   if (info.count_app > 0) {
-    cudaError_t e = app_level(p, s, info, maxkids, prm, vals, diag, stream, prof);
+    cudaError_t e = app_level(p, s, info, prm, vals, diag, stream, prof);
     if (e != cudaSuccess) return e;
   }
   if (info.count_large == 0) {
@@ -873,15 +900,8 @@ cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevel
   const size_t smem = (size_t)R * (2 * (NB + 1) + 2) * sizeof(double);
   const int steps = (info.max_fs_large + (NB - 2)) / (NB - 1) + 1;
   {
-    const int nl = info.count_large;
-    const int ych = std::min(256, (info.max_f + 7) / 8);
-    prof.begin(stream);
-    big_zero_kernel<<<dim3(nl, ych), 256, 0, stream>>>(s, list5);
-    big_scatter_kernel<<<dim3(nl, 16), 256, 0, stream>>>(p, s, vals, diag, list5);
-    if (diag) big_diag_kernel<<<nl, 256, 0, stream>>>(p, s, diag, list5);
-    for (int c = 0; c < maxkids; c++)
-      big_extend_kernel<<<dim3(nl, ych), 256, 0, stream>>>(p, s, c, list5);
-    prof.end(kPhBigAsm, stream, 2 + (diag ? 1 : 0) + maxkids);
+    cudaError_t e = assemble_big(p, s, list5, info.count_large, vals, diag, stream, prof);
+    if (e != cudaSuccess) return e;
   }
   const int upd_grid = 148 * 4;
   const int cnb = big_chain_panel_width(info.max_f_large);

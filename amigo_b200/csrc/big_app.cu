@@ -271,26 +271,45 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
       const int a = xi[kIDpos + q];
       const int b = ncand - 1;
       if (a < b) {
-        for (int j = lane; j < f; j += 32) {
-          double *p, *r;
-          if (j < a) {
-            p = F + a + (size_t)f * j;
-            r = F + b + (size_t)f * j;
-          } else if (j == a) {
-            p = F + a + (size_t)f * a;
-            r = F + b + (size_t)f * b;
-          } else if (j < b) {
-            p = F + j + (size_t)f * a;
-            r = F + b + (size_t)f * j;
-          } else if (j == b) {
-            continue;
-          } else {
-            p = F + j + (size_t)f * a;
-            r = F + j + (size_t)f * b;
+        // the pairs of a symmetric interchange are distinct entries: eight
+        // passes of the warp load theirs before any is stored back
+        constexpr int kU = 8;
+        for (int j0 = 0; j0 < f; j0 += 32 * kU) {
+          double* p[kU];
+          double* r[kU];
+          double vp[kU], vr[kU];
+#pragma unroll
+          for (int u = 0; u < kU; u++) {
+            const int j = j0 + 32 * u + lane;
+            p[u] = nullptr;
+            r[u] = nullptr;
+            if (j >= f || j == b) continue;
+            if (j < a) {
+              p[u] = F + a + (size_t)f * j;
+              r[u] = F + b + (size_t)f * j;
+            } else if (j == a) {
+              p[u] = F + a + (size_t)f * a;
+              r[u] = F + b + (size_t)f * b;
+            } else if (j < b) {
+              p[u] = F + j + (size_t)f * a;
+              r[u] = F + b + (size_t)f * j;
+            } else {
+              p[u] = F + j + (size_t)f * a;
+              r[u] = F + j + (size_t)f * b;
+            }
           }
-          const double t = *p;
-          *p = *r;
-          *r = t;
+#pragma unroll
+          for (int u = 0; u < kU; u++) {
+            vp[u] = p[u] ? *p[u] : 0.0;
+            vr[u] = p[u] ? *r[u] : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < kU; u++) {
+            if (p[u]) {
+              *p[u] = vr[u];
+              *r[u] = vp[u];
+            }
+          }
         }
         if (lane == 0) {
           int t = fv[a];

@@ -192,8 +192,7 @@ void launch_factor_level(const DevPlan& p, const DevState& s,
 cudaError_t configure_factor_kernels();
 size_t factor_smem_bytes();
 
-// Big-front pipeline for one level (see big.cu). `maxkids` is the largest
-// number of children among the level's supernodes.
+// Big-front pipeline for one level (see big.cu).
 struct BigLevelInfo {
   int count, max_f, max_fs;
   int count_large, max_fs_large;
@@ -231,7 +230,7 @@ cudaError_t launch_app_level(const DevState& s, const FactorParams& prm, int cou
 cudaError_t configure_app_kernels();
 
 cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
-                             int maxkids, const FactorParams& prm, const double* vals,
+                             const FactorParams& prm, const double* vals,
                              const double* diag, cudaStream_t stream, Prof& prof);
 cudaError_t configure_big_kernels();
 
