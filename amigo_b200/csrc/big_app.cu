@@ -100,23 +100,32 @@ __device__ __forceinline__ double fsym(const double* F, int f, int a, int b) {
 
 __device__ __forceinline__ int* xint(double* X) { return reinterpret_cast<int*>(X + kXInt); }
 
-// largest value, lowest index on ties (idamax)
-__device__ __forceinline__ void warp_argmax(double& v, int& i) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const double ov = __shfl_xor_sync(0xffffffffu, v, o);
-    const int oi = __shfl_xor_sync(0xffffffffu, i, o);
-    if (ov > v || (ov == v && oi < i)) {
-      v = ov;
-      i = oi;
-    }
-  }
+// Non-negative doubles order as their bit patterns, so the warp reductions
+// below are exact integer reductions (redux.sync) on the high and then the
+// low 32 bits, instead of FP64 shuffle butterflies.
+
+// Largest of the non-negative values v of the lanes with `on`, and the
+// lowest lane holding it (idamax); -1 and lane 0 when no lane is on.
+__device__ __forceinline__ void warp_argmax(bool on, double v, double& best, int& idx) {
+  const unsigned long long b = on ? (unsigned long long)__double_as_longlong(v) : 0ull;
+  // +1 keeps an active 0.0 above the inactive lanes
+  const unsigned hi = on ? (unsigned)(b >> 32) + 1u : 0u;
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const bool cand = on && hi == mhi;
+  const unsigned lo = cand ? (unsigned)b : 0u;
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, lo);
+  const unsigned win = __ballot_sync(0xffffffffu, cand && lo == mlo);
+  idx = win ? __ffs(win) - 1 : 0;
+  best = mhi ? __longlong_as_double((long long)(((unsigned long long)(mhi - 1u) << 32) | mlo))
+             : -1.0;
 }
 
+// largest of the lanes' non-negative values
 __device__ __forceinline__ double warp_max(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
+  const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, (unsigned)(b >> 32));
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, (unsigned)(b >> 32) == mhi ? (unsigned)b : 0u);
+  return __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
 }
 
 // ------------------------------------------------------------- shared memory
@@ -383,9 +392,9 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
     const double wkk = w.A[t][t];
     const bool has = t + 1 < nr;
     const double at = fabs(w.A[lane][t]);
-    double bv = (lane > t && lane < nr) ? at : -1.0;
-    int bi = lane;
-    warp_argmax(bv, bi);
+    double bv;
+    int bi;
+    warp_argmax(lane > t && lane < nr, at, bv, bi);
     const double abswik = has ? bv : 0.0;
     const int imax = has ? bi : t;
     // block rows that are not candidates any more (rotated behind)
