@@ -387,11 +387,26 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
   // a pivot accepted before it. Accepted pivots are checked with the exact
   // maxima in phase A.
   const double u = prm.ustab, tol = prm.pivot_tol;
+  constexpr unsigned kFull = 0xffffffffu;
   int t = 0, nr = nbk;
+  // Left-looking: the block keeps its entries as loaded in the columns not
+  // pivoted yet, next to the pivot columns (W) and the L rows of the pivots
+  // taken. A column that a test reads is formed when it is read: entry
+  // (i, j) minus L(max(i, j), q) W(min(i, j), q) for each earlier pivot q in
+  // order, the products and the order of the reference's lower-triangle
+  // update. Lane i forms row i.
+  auto form = [&](int j) -> double {
+    if (lane < t || lane >= nbk) return 0.0;
+    const int hi = max(lane, j), lo = min(lane, j);
+    double v = w.A[lane][j];
+    for (int q = 0; q < t; q++) v = fma(-w.Lb[hi][q], w.A[lo][q], v);
+    return v;
+  };
   while (t < nr) {
-    const double wkk = w.A[t][t];
     const bool has = t + 1 < nr;
-    const double at = fabs(w.A[lane][t]);
+    const double ct = form(t);  // the candidate's column
+    const double wkk = __shfl_sync(kFull, ct, t);
+    const double at = fabs(ct);
     double bv;
     int bi;
     warp_argmax(lane > t && lane < nr, at, bv, bi);
@@ -403,6 +418,7 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
     const double colmax = fmax(col_in, t == 0 ? w.below0[w.perm[t]] : 0.0);
     int stp = 0, kpiv = t;
     double row_in = 0.0;
+    double c2 = 0.0;  // the column of the partner or of imax, when formed
     // a pair that formed a 2x2 pivot in the pivot record is tried as that
     // 2x2 first (the Duff test), since a 1x1 test that sees only the block's
     // rows would accept the first of them alone and the a-posteriori test
@@ -413,10 +429,10 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
       hinted = w.var[pt] >= 0 && vn >= 0 && w.part[pt] == vn;
     }
     if (hinted) {
-      const double r2 =
-          warp_max((lane >= t && lane < nbk && lane != t + 1) ? fabs(w.A[lane][t + 1]) : 0.0);
+      c2 = form(t + 1);
+      const double r2 = warp_max((lane >= t && lane < nbk && lane != t + 1) ? fabs(c2) : 0.0);
       const double rm2 = fmax(r2, t == 0 ? w.below0[w.perm[t + 1]] : 0.0);
-      const double w21 = w.A[t + 1][t], w22 = w.A[t + 1][t + 1];
+      const double w21 = __shfl_sync(kFull, ct, t + 1), w22 = __shfl_sync(kFull, c2, t + 1);
       const double det = fabs(wkk * w22 - w21 * w21);
       if (det >= tol) {
         const double delta = det / fmax(fabs(w22) + fabs(w21), fabs(wkk) + fabs(w21));
@@ -432,9 +448,10 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
     } else if (fabs(wkk) >= tol && fabs(wkk) >= u * colmax) {
       stp = 1;
     } else if (has) {
-      row_in = warp_max((lane >= t && lane < nbk && lane != imax) ? fabs(w.A[lane][imax]) : 0.0);
+      c2 = form(imax);
+      row_in = warp_max((lane >= t && lane < nbk && lane != imax) ? fabs(c2) : 0.0);
       const double rowmax = fmax(row_in, t == 0 ? w.below0[w.perm[imax]] : 0.0);
-      const double wii = w.A[imax][imax], wik = w.A[imax][t];
+      const double wii = __shfl_sync(kFull, c2, imax), wik = __shfl_sync(kFull, ct, imax);
       if (fabs(wii) >= tol && fabs(wii) >= u * rowmax) {
         stp = 1;
         kpiv = imax;
@@ -484,9 +501,18 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
       nr--;
       continue;
     }
+    // the pivot columns at their positions after the interchange (rows
+    // ksrc and kdst exchanged), stored as W for the later columns
+    const int src = (lane == ksrc) ? kdst : (lane == kdst) ? ksrc : lane;
+    const double p1 = __shfl_sync(kFull, (stp == 1 && kpiv != t) ? c2 : ct, src);
+    const double p2 = __shfl_sync(kFull, c2, src);
+    if (lane >= t && lane < nbk) {
+      w.A[lane][t] = p1;
+      if (stp == 2) w.A[lane][t + 1] = p2;
+    }
     if (stp == 1) {
-      const double d = w.A[t][t];
-      const double li = w.A[lane][t] * (1.0 / d);
+      const double d = __shfl_sync(kFull, p1, t);
+      const double li = p1 * (1.0 / d);
       if (lane > t && lane < nbk) w.Lb[lane][t] = li;
       if (lane == 0) {
         w.kind[t] = 1;
@@ -494,13 +520,13 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
         w.cin[t] = (kpiv == t) ? col_in : row_in;
       }
     } else {
-      const double d11 = w.A[t][t], d21 = w.A[t + 1][t], d22 = w.A[t + 1][t + 1];
+      const double d11 = __shfl_sync(kFull, p1, t), d21 = __shfl_sync(kFull, p1, t + 1),
+                   d22 = __shfl_sync(kFull, p2, t + 1);
       const double di = 1.0 / (d11 * d22 - d21 * d21);
       const double i00 = d22 * di, i01 = -d21 * di, i11 = d11 * di;
-      const double a = w.A[lane][t], b = w.A[lane][t + 1];
       if (lane > t + 1 && lane < nbk) {
-        w.Lb[lane][t] = a * i00 + b * i01;
-        w.Lb[lane][t + 1] = a * i01 + b * i11;
+        w.Lb[lane][t] = p1 * i00 + p2 * i01;
+        w.Lb[lane][t + 1] = p1 * i01 + p2 * i11;
       }
       if (lane == 0) {
         w.kind[t] = 2;
@@ -513,24 +539,7 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
       }
     }
     __syncwarp();
-    // rank-1 or rank-2 update of the block's remaining rows and columns
-    // (rotated ones included): entry (i, j) gets L(max) W(min) in both
-    // triangles, the lower-triangle product of the reference's update. The
-    // column loop is unrolled so that its loads are in flight together.
-    const int t1 = t + stp;
-    if (lane >= t1 && lane < nbk) {
-#pragma unroll
-      for (int c = 0; c < kBlk; c++) {
-        if (c >= t1 && c < nbk) {
-          const int hi = max(lane, c), lo = min(lane, c);
-          double v = w.A[lane][c] - w.Lb[hi][t] * w.A[lo][t];
-          if (stp == 2) v -= w.Lb[hi][t + 1] * w.A[lo][t + 1];
-          w.A[lane][c] = v;
-        }
-      }
-    }
-    __syncwarp();
-    t = t1;
+    t += stp;
   }
   const int acc = t;
   const bool moved = __ballot_sync(0xffffffffu, lane < nbk && w.perm[lane] != lane) != 0u;
