@@ -303,16 +303,17 @@ void build_plan(b200ldl_t h, const int* rowp, const int* cols) {
 
   // pool estimates from the symbolic fronts, scaled by the delay growth; a
   // structure re-planned from a pivot record already holds its delays, and
-  // its big fronts other than roots take the a-posteriori panels, which need
-  // no chained-panel scratch
+  // its big fronts take the a-posteriori panels, which need no chained-panel
+  // scratch except at roots (which may finish with chained panels)
   double ints = 0.0, dbl = 0.0;
   for (int k = 0; k < nn; k++) {
     const double f = h->h_ns[k] + h->h_nc[k];
     ints += 2.0 * f;
     dbl += f * h->h_ns[k] + (double)h->h_nc[k] * h->h_nc[k];
     if (f > kSmemFrontMax) dbl += f * f + (kBigPanelMax + 2.0) * f + kAppScratch;
-    if (f > cluster_front_limit(4) && !(h->replanned && h->h_nc[k] > 0))
-      dbl += f * f + 32.0 * f;  // chained panels' scratch
+    const bool chain = h->replanned ? (f > kSmemFrontMax && h->h_nc[k] == 0)
+                                    : f > cluster_front_limit(4);
+    if (chain) dbl += f * f + 32.0 * f;  // chained panels' scratch
   }
   const double g = h->replanned ? 1.0 : std::max(1.0, h->delay_growth);
   h->icap = (unsigned long long)(ints * g * 1.5) + (1u << 16);
@@ -454,7 +455,7 @@ void upload_plan(b200ldl_t h) {
   CK(h->d_used.alloc(3));
   CK(h->d_big.alloc(nn));
   CK(h->d_big_meta.alloc(kBigMeta));
-  CK(h->d_class_list.alloc((size_t)7 * std::max(1, nn)));
+  CK(h->d_class_list.alloc((size_t)8 * std::max(1, nn)));
   h->uploaded = true;
 }
 

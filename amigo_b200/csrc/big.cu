@@ -824,8 +824,47 @@ cudaError_t assemble_big(const DevPlan& p, const DevState& s, const int* list, i
   return e;
 }
 
+// Panels and trailing updates of the fronts in `list` from their current
+// position (B.k), at most `max_left` candidates left per front: a chained
+// panel per launch where the front fits the chained kernel, else the
+// per-pivot panel kernel.
+cudaError_t run_big_panels(const DevState& s, const FactorParams& prm, const int* list, int count,
+                           int max_f, int max_left, cudaStream_t stream, Prof& prof) {
+  const int CL = max_f > 1600 ? 16 : 8;
+  const int R = (max_f + CL - 1) / CL;
+  int NB = kBigPanelMax;
+  while (NB > 4 && (size_t)R * (2 * (NB + 1) + 2) * sizeof(double) > kPanelSmemMax) NB >>= 1;
+  const size_t smem = (size_t)R * (2 * (NB + 1) + 2) * sizeof(double);
+  const int upd_grid = 148 * 4;
+  const int cnb = big_chain_panel_width(max_f);
+  const bool chained = cnb > 0;
+  const int nsteps = chained ? (max_left + cnb - 2) / (cnb - 1) + 1
+                             : (max_left + (NB - 2)) / (NB - 1) + 1;
+  for (int st = 0; st < nsteps; st++) {
+    cudaError_t e;
+    prof.begin(stream);
+    if (chained)
+      e = launch_big_chain_panel(s, prm, count, max_f, cnb, list, stream);
+    else if (CL == 16)
+      e = launch_panel<16>(s, prm, count, NB, smem, list, stream);
+    else
+      e = launch_panel<8>(s, prm, count, NB, smem, list, stream);
+    if (e != cudaSuccess) return e;
+    prof.end(kPhBigPanel, stream, 1);
+    prof.begin(stream);
+    for (int c0 = 0; c0 < count; c0 += kUpdMaxFronts) {
+      const int nl = std::min(kUpdMaxFronts, count - c0);
+      big_update_kernel<<<upd_grid, kUpdThreads, 0, stream>>>(s, list + c0, nl);
+    }
+    prof.end(kPhBigUpd, stream, (count + kUpdMaxFronts - 1) / kUpdMaxFronts);
+  }
+  return cudaGetLastError();
+}
+
 // Class-6 fronts: blocked panels with a-posteriori tests (big_app.cu), all
-// of the level's panel steps in one cooperative launch.
+// of the level's panel steps in one cooperative launch. Roots among them
+// whose panels left candidates (failed tests cannot be delayed past a root)
+// finish with the chained panels, Bunch-Kaufman as for every root.
 cudaError_t app_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
                       const FactorParams& prm, const double* vals,
                       const double* diag, cudaStream_t stream, Prof& prof) {
@@ -834,15 +873,18 @@ cudaError_t app_level(const DevPlan& p, const DevState& s, const BigLevelInfo& i
   cudaError_t e = assemble_big(p, s, list6, nl, vals, diag, stream, prof);
   if (e != cudaSuccess) return e;
   prof.begin(stream);
-  e = launch_app_level(s, prm, nl, info.max_fs_app, list6, s.big_meta + 21, stream);
+  int* list7 = s.class_list + (size_t)7 * p.num_nodes;
+  e = launch_app_level(s, prm, nl, info.max_fs_app, list6, list7, s.big_meta, stream);
   if (e != cudaSuccess) return e;
   prof.end(kPhBigPanel, stream, 1);
-  int cap = 0;
-  e = cudaMemcpyAsync(&cap, s.big_meta + 23, sizeof(int), cudaMemcpyDeviceToHost, stream);
+  int meta[5] = {0, 0, 0, 0, 0};  // big_meta[19..23]
+  e = cudaMemcpyAsync(meta, s.big_meta + 19, sizeof(meta), cudaMemcpyDeviceToHost, stream);
   if (e != cudaSuccess) return e;
   e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) return e;
-  return cap ? cudaErrorUnknown : cudaSuccess;
+  if (meta[4]) return cudaErrorUnknown;  // the step cap or a tensor-core timeout
+  if (meta[0] > 0) return run_big_panels(s, prm, list7, meta[0], info.max_f_app, meta[1], stream, prof);
+  return cudaSuccess;
 }
 
 }  // namespace
@@ -891,40 +933,14 @@ cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevel
     return cudaGetLastError();
   }
   // larger fronts: a cluster per front, one panel per launch over the front
-  // in global memory; <= 200 rows per CTA where possible
+  // in global memory
   const int* list5 = s.class_list + (size_t)5 * p.num_nodes;
-  int CL = info.max_f > 1600 ? 16 : 8;
-  const int R = (info.max_f + CL - 1) / CL;
-  int NB = kBigPanelMax;
-  while (NB > 4 && (size_t)R * (2 * (NB + 1) + 2) * sizeof(double) > kPanelSmemMax) NB >>= 1;
-  const size_t smem = (size_t)R * (2 * (NB + 1) + 2) * sizeof(double);
-  const int steps = (info.max_fs_large + (NB - 2)) / (NB - 1) + 1;
   {
     cudaError_t e = assemble_big(p, s, list5, info.count_large, vals, diag, stream, prof);
     if (e != cudaSuccess) return e;
-  }
-  const int upd_grid = 148 * 4;
-  const int cnb = big_chain_panel_width(info.max_f_large);
-  const bool chained = cnb > 0;
-  const int nsteps = chained ? (info.max_fs_large + cnb - 2) / (cnb - 1) + 1 : steps;
-  for (int st = 0; st < nsteps; st++) {
-    cudaError_t e;
-    prof.begin(stream);
-    if (chained)
-      e = launch_big_chain_panel(s, prm, info.count_large, info.max_f_large, cnb, list5,
-                                 stream);
-    else if (CL == 16)
-      e = launch_panel<16>(s, prm, info.count_large, NB, smem, list5, stream);
-    else
-      e = launch_panel<8>(s, prm, info.count_large, NB, smem, list5, stream);
+    e = run_big_panels(s, prm, list5, info.count_large, info.max_f_large, info.max_fs_large,
+                       stream, prof);
     if (e != cudaSuccess) return e;
-    prof.end(kPhBigPanel, stream, 1);
-    prof.begin(stream);
-    for (int c0 = 0; c0 < info.count_large; c0 += kUpdMaxFronts) {
-      const int nl = std::min(kUpdMaxFronts, info.count_large - c0);
-      big_update_kernel<<<upd_grid, kUpdThreads, 0, stream>>>(s, list5 + c0, nl);
-    }
-    prof.end(kPhBigUpd, stream, (info.count_large + kUpdMaxFronts - 1) / kUpdMaxFronts);
   }
   prof.begin(stream);
   big_finalize_kernel<<<(nb + 255) / 256, 256, 0, stream>>>(s, nb, prm.cholesky);

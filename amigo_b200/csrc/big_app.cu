@@ -244,11 +244,26 @@ __device__ __forceinline__ int item_front(const Prefix& P, int nl, long long t) 
 
 // ---------------------------------------------------------------- phase D
 
+// A front whose candidates are all decided is done, except a root with
+// candidates left (delayed by the tests; a root has no parent to take them):
+// they become candidates again and the root waits in `done` for the chained
+// panels (Bunch-Kaufman) that run after this launch.
+__device__ void finish_front(const DevState& s, BigFront* B, int* done, int* meta) {
+  if (B->nc == 0 && B->k < B->fs) {
+    B->ncand = B->fs;
+    B->state = 3;
+    done[atomicAdd(meta + 19, 1)] = (int)(B - s.big);
+    atomicMax(meta + 20, B->fs - B->k);
+  } else {
+    B->state = 2;
+  }
+}
+
 // Close the previous step of front B (trailing-update work counters, a
 // finished front becomes done), apply the delays it left, and factor the
 // next diagonal block. Returns 1 if the front takes part in this step.
 __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFront* B, int step,
-                             WarpDiag& w) {
+                             WarpDiag& w, int* done, int* meta) {
   const int lane = threadIdx.x & 31;
   const int f = B->f;
   double* F = s.dpool + B->doff;
@@ -267,7 +282,7 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
   __syncwarp();
   if (lane == 0) {
     B->kw = 0;
-    if (B->state == 1) B->state = 2;
+    if (B->state == 1) finish_front(s, B, done, meta);
   }
   __syncwarp();
   if (B->pending > 0 && B->state == 0) {
@@ -338,7 +353,7 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
     if (lane == 0) {
       B->ncand = ncand;
       B->pending = 0;
-      if (B->k >= ncand) B->state = 2;
+      if (B->k >= ncand) finish_front(s, B, done, meta);
     }
     __syncwarp();
   }
@@ -943,7 +958,8 @@ __device__ int phase_u_tile_mixed(const DevState& s, const BigFront& B, int I, i
 
 __global__ void __launch_bounds__(kThreads, 1)
     app_level_kernel(DevState s, FactorParams prm, const int* __restrict__ list, int nl,
-                     int max_steps, int* counters) {
+                     int max_steps, int* done, int* meta) {
+  int* counters = meta + 21;
   cg::grid_group grid = cg::this_grid();
   extern __shared__ __align__(1024) unsigned char dsm[];
   __shared__ Prefix P;
@@ -971,7 +987,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       WarpDiag& w = reinterpret_cast<WarpDiag*>(dsm)[warp];
       if (blockIdx.x == 0 && tid == 0) counters[(step + 1) & 1] = 0;
       for (int i = gwarp; i < nl; i += nwarp) {
-        const int on = phase_d_front(s, prm, s.big + list[i], step, w);
+        const int on = phase_d_front(s, prm, s.big + list[i], step, w, done, meta);
         if (on && (tid & 31) == 0) atomicAdd(counters + (step & 1), 1);
       }
     }
@@ -1034,6 +1050,12 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   // the step cap (never reached when every step makes progress)
   if (step > max_steps && blockIdx.x == 0 && tid == 0) counters[2] = 1;
+  // every CTA has left the loop: the roots set aside take part in the
+  // chained panels that follow
+  if (blockIdx.x == 0) {
+    const int nd = *((volatile int*)(meta + 19));
+    for (int i = tid; i < nd; i += kThreads) s.big[done[i]].state = 0;
+  }
   if (prm.mixed) {
     if (tc_fail) {
       // a tensor-core operation did not complete in time: the factorization
@@ -1050,7 +1072,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 }  // namespace
 
 cudaError_t launch_app_level(const DevState& s, const FactorParams& prm, int count, int max_fs,
-                             const int* list, int* counters, cudaStream_t stream) {
+                             const int* list, int* done, int* meta, cudaStream_t stream) {
   static_assert(kBlk == kBigPanelMax, "panel width");
   if (count <= 0) return cudaSuccess;
   int dev = 0, nsm = 0, per = 0;
@@ -1068,8 +1090,10 @@ cudaError_t launch_app_level(const DevState& s, const FactorParams& prm, int cou
   FactorParams pa = prm;
   const int* la = list;
   int na = count;
-  int* ca = counters;
-  void* args[] = {(void*)&sa, (void*)&pa, (void*)&la, (void*)&na, (void*)&max_steps, (void*)&ca};
+  int* da = done;
+  int* ma = meta;
+  void* args[] = {(void*)&sa, (void*)&pa,        (void*)&la, (void*)&na,
+                  (void*)&max_steps, (void*)&da, (void*)&ma};
   return cudaLaunchCooperativeKernel((const void*)app_level_kernel, dim3(grid), dim3(kThreads),
                                      args, kDynSmem, stream);
 }

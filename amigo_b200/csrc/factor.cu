@@ -156,10 +156,14 @@ __global__ void __launch_bounds__(kFactorThreads)
       // on-chip limit also get the chained panel's W by physical row and its
       // permutation scratch
       unsigned long long need = (unsigned long long)f * f + (unsigned long long)kBigPanelMax * f;
-      if (prm.app && nc > 0 && f >= prm.app_min_f)
-        need += (unsigned long long)kAppScratch;
-      else if (f > s.cf_limit[4])
-        need += (unsigned long long)kBigPanelMax * f + (unsigned long long)(fs + 1) * f;
+      const unsigned long long chain =
+          (unsigned long long)kBigPanelMax * f + (unsigned long long)(fs + 1) * f;
+      if (prm.app && f >= prm.app_min_f) {
+        // a root may finish with the chained panels: their scratch too
+        need += (unsigned long long)kAppScratch + (nc == 0 ? chain : 0ull);
+      } else if (f > s.cf_limit[4]) {
+        need += chain;
+      }
       const unsigned long long dofs = atomicAdd(s.used + 1, need);
       if (dofs + need > s.dcap) fail = 1;
       sh_doff = (long long)dofs;
@@ -194,7 +198,7 @@ __global__ void __launch_bounds__(kFactorThreads)
       const int slot = atomicAdd(s.big_meta, 1);
       atomicMax(s.big_meta + 1, f);
       atomicMax(s.big_meta + 2, fs);
-      const bool app = prm.app && nc > 0 && f >= prm.app_min_f;
+      const bool app = prm.app && f >= prm.app_min_f;
       int cls = 5;
       if (app) {
         cls = 6;
@@ -237,7 +241,10 @@ __global__ void __launch_bounds__(kFactorThreads)
       b.ioff = sh_ioff;
       b.doff = sh_doff;
       b.woff = sh_doff + (long long)f * f;
-      b.xoff = b.woff + (long long)kBigPanelMax * f;
+      // a-posteriori scratch after the panel's W (and, for a root, after the
+      // chained panels' scratch)
+      b.xoff = b.woff + (long long)kBigPanelMax * f +
+               ((app && nc == 0) ? (long long)kBigPanelMax * f + (long long)(fs + 1) * f : 0ll);
       b.flops = 0.0;
       s.big[slot] = b;
     }

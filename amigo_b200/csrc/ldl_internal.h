@@ -157,8 +157,10 @@ struct DevState {
   int* big_meta;    // [kBigMeta]: count, max f, max fs, count large, max fs
                     // large, class counts [5..9], class max f [10..14], max f
                     // large [15], a-posteriori fronts: count [16], max f [17],
-                    // max fs [18], their step counters and cap flag [21..23]
-  int* class_list;  // [7][nn] big-front indices per size class (6: a-posteriori)
+                    // max fs [18], roots left with candidates: count [19], most
+                    // candidates left [20], step counters and failure flag [21..23]
+  int* class_list;  // [8][nn] big-front indices per size class (6: a-posteriori,
+                    // 7: a-posteriori roots that finish with chained panels)
   int cf_limit[5];  // largest front of each on-chip class
   // fronts re-planned from a pivot record: partner[v] = the variable that
   // formed a 2x2 pivot with v in the record, -1 otherwise (nullptr without a
@@ -225,8 +227,11 @@ cudaError_t launch_big_chain_panel(const DevState& s, const FactorParams& prm, i
 // one cooperative launch. counters: 3 zeroed ints in device memory;
 // counters[2] is set if the step cap was reached (it is not when every step
 // makes progress).
+// `done` receives the roots whose panels left candidates (count in
+// meta[19], most candidates left in meta[20]); meta[21..22] are the step
+// counters and meta[23] the failure flag.
 cudaError_t launch_app_level(const DevState& s, const FactorParams& prm, int count, int max_fs,
-                             const int* list, int* counters, cudaStream_t stream);
+                             const int* list, int* done, int* meta, cudaStream_t stream);
 cudaError_t configure_app_kernels();
 
 cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevelInfo& info,
