@@ -91,7 +91,9 @@ constexpr int kINcand = 100;
 constexpr int kIMoved = 101;  // 1 if the block permutation is not the identity
 constexpr int kIDcnt = 102;   // candidates to delay at the next step
 constexpr int kIDpos = 103;   // [32] their positions, decreasing
-constexpr int kINint = kIDpos + kBlk;
+constexpr int kINp = kIDpos + kBlk;  // pivots that pass the exact tests (set by phase R)
+constexpr int kIRdone = kINp + 1;    // phase-R items of the panel finished
+constexpr int kINint = kIRdone + 1;
 static_assert(kXInt + (kINint + 1) / 2 <= kAppScratch, "a-posteriori scratch size");
 
 __device__ __forceinline__ double fsym(const double* F, int f, int a, int b) {
@@ -176,6 +178,8 @@ __device__ int passing_prefix(const RowsSm& sm, int acc, double ustab, double to
 struct UpdSm {  // phase U
   double As[kBigPanelMax][kTileU];
   double Bs[kBigPanelMax][kTileU];
+  double ud[3 * kBlk], usinv[kBlk];  // the panel's D, when L is formed from W
+  int ukind[kBlk];
 };
 
 struct Prefix {  // work items of up to kChunkFronts fronts
@@ -259,32 +263,40 @@ __device__ void finish_front(const DevState& s, BigFront* B, int* done, int* met
   }
 }
 
+template <int NT>
+__device__ __forceinline__ void group_sync() {
+  if constexpr (NT == 32)
+    __syncwarp();
+  else
+    __syncthreads();
+}
+
 // Close the previous step of front B (trailing-update work counters, a
-// finished front becomes done), apply the delays it left, and factor the
-// next diagonal block. Returns 1 if the front takes part in this step.
-__device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFront* B, int step,
-                             WarpDiag& w, int* done, int* meta) {
-  const int lane = threadIdx.x & 31;
+// finished front becomes done) and apply the delays it left, by a group of
+// NT threads (a warp, or the CTA when the level has no more fronts than
+// CTAs); g is the thread's index in the group. Returns 1 if the front takes
+// part in this step.
+template <int NT>
+__device__ int phase_d_prepare(const DevState& s, BigFront* B, int* done, int* meta, int g) {
   const int f = B->f;
   double* F = s.dpool + B->doff;
-  double* Wg = s.dpool + B->woff;
   double* X = s.dpool + B->xoff;
   int* xi = xint(X);
   int* fv = s.ivars + B->ioff;
   int* orig = fv + f;
-  if (lane == 0 && B->kw > 0) {
+  if (g == 0 && B->kw > 0) {
     const double r = (double)(f - B->k);
     const double fl = r * (r + 1.0) * B->kw;
     B->flops += fl;
     atomicAdd(s.flops + 2, fl);
     atomicAdd(s.flops + 3, 8.0 * (r * (r + 1.0) + 2.0 * r * B->kw));
   }
-  __syncwarp();
-  if (lane == 0) {
+  group_sync<NT>();
+  if (g == 0) {
     B->kw = 0;
     if (B->state == 1) finish_front(s, B, done, meta);
   }
-  __syncwarp();
+  group_sync<NT>();
   if (B->pending > 0 && B->state == 0) {
     // the candidates to delay move behind the remaining candidates, largest
     // position first so that no interchange moves another one still to go
@@ -296,15 +308,15 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
       const int b = ncand - 1;
       if (a < b) {
         // the pairs of a symmetric interchange are distinct entries: eight
-        // passes of the warp load theirs before any is stored back
+        // passes of the group load theirs before any is stored back
         constexpr int kU = 8;
-        for (int j0 = 0; j0 < f; j0 += 32 * kU) {
+        for (int j0 = 0; j0 < f; j0 += NT * kU) {
           double* p[kU];
           double* r[kU];
           double vp[kU], vr[kU];
 #pragma unroll
           for (int u = 0; u < kU; u++) {
-            const int j = j0 + 32 * u + lane;
+            const int j = j0 + NT * u + g;
             p[u] = nullptr;
             r[u] = nullptr;
             if (j >= f || j == b) continue;
@@ -335,7 +347,7 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
             }
           }
         }
-        if (lane == 0) {
+        if (g == 0) {
           int t = fv[a];
           fv[a] = fv[b];
           fv[b] = t;
@@ -348,16 +360,29 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
         }
       }
       ncand--;
-      __syncwarp();
+      group_sync<NT>();
     }
-    if (lane == 0) {
+    if (g == 0) {
       B->ncand = ncand;
       B->pending = 0;
       if (B->k >= ncand) finish_front(s, B, done, meta);
     }
-    __syncwarp();
+    group_sync<NT>();
   }
-  if (B->state != 0) return 0;
+  return B->state == 0 ? 1 : 0;
+}
+
+// Factor the next diagonal block of front B (one warp). Returns 1.
+__device__ int phase_d_block(const DevState& s, const FactorParams& prm, BigFront* B, int step,
+                             WarpDiag& w) {
+  const int lane = threadIdx.x & 31;
+  const int f = B->f;
+  double* F = s.dpool + B->doff;
+  double* Wg = s.dpool + B->woff;
+  double* X = s.dpool + B->xoff;
+  int* xi = xint(X);
+  int* fv = s.ivars + B->ioff;
+  int* orig = fv + f;
 
   const int k = B->k;
   const int ncand = B->ncand;
@@ -392,6 +417,8 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
   w.dd[3 * lane] = w.dd[3 * lane + 1] = w.dd[3 * lane + 2] = 0.0;
   w.below0[lane] = __longlong_as_double(
       (long long)reinterpret_cast<unsigned long long*>(X + kXNext)[lane]);
+  // read: the trailing update of this panel fills them again for the next
+  X[kXNext + lane] = 0.0;
   __syncwarp();
 
   // The reference's tests on the block's candidates in order. For the
@@ -571,6 +598,7 @@ __device__ int phase_d_front(const DevState& s, const FactorParams& prm, BigFron
   xi[kIKind + lane] = w.kind[lane];
   xi[kIDlt + lane] = w.dlt[lane];
   if (lane == 0) {
+    xi[kIRdone] = 0;
     xi[kIAcc] = acc;
     xi[kINbk] = nbk;
     xi[kIK] = k;
@@ -621,13 +649,13 @@ __device__ __forceinline__ int row_chunks(const DevState& s, const BigFront& B, 
   return max(1, (rows + kThreads - 1) / kThreads);
 }
 
-__device__ void phase_r_item(const DevState& s, const BigFront& B, int chunk, int nchunk,
-                             RowsSm& sm) {
+__device__ void phase_r_item(const DevState& s, const FactorParams& prm, const BigFront& B,
+                             int chunk, int nchunk, RowsSm& sm) {
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
   double* X = s.dpool + B.xoff;
-  const int* xi = xint(X);
+  int* xi = xint(X);
   const int f = B.f;
   const int k = xi[kIK];
   const int nbk = xi[kINbk];
@@ -689,10 +717,44 @@ __device__ void phase_r_item(const DevState& s, const BigFront& B, int chunk, in
       atomicMax(reinterpret_cast<unsigned long long*>(X + kXBelow) + tid,
                 (unsigned long long)__double_as_longlong(v));
   }
+  // the front's last item to finish has the column maxima over the whole
+  // front: it runs the reference's tests on the block's pivots and records
+  // how many pass (kINp), for the commit and the trailing update
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) sm.np = (atomicAdd(xi + kIRdone, 1) == nchunk - 1) ? 1 : 0;
+  __syncthreads();
+  if (sm.np) {
+    __threadfence();
+    if (tid < kBlk) {
+      sm.skind[tid] = xi[kIKind + tid];
+      sm.sd[3 * tid] = X[kXD + 3 * tid];
+      sm.sd[3 * tid + 1] = X[kXD + 3 * tid + 1];
+      sm.sd[3 * tid + 2] = X[kXD + 3 * tid + 2];
+      const unsigned long long bl =
+          *(reinterpret_cast<volatile unsigned long long*>(X + kXBelow) + tid);
+      sm.scm[tid] = fmax(X[kXCin + tid], __longlong_as_double((long long)bl));
+      sm.srm[tid] = X[kXRin + tid];
+    }
+    __syncthreads();
+    if (tid == 0) xi[kINp] = passing_prefix(sm, acc, prm.ustab, prm.pivot_tol);
+  }
   __syncthreads();
 }
 
 // ---------------------------------------------------------------- phase A
+
+// The L entries (l0, l1) of a row whose W entries are (a, b) under the 2x2
+// pivot d = (d11, d21, d22): (a, b) D^-1, with explicit fused multiply-adds so
+// that every kernel that forms them gets the same values.
+__device__ __forceinline__ void l_2x2(const double* d, double a, double b, double& l0,
+                                      double& l1) {
+  const double d11 = d[0], d21 = d[1], d22 = d[2];
+  const double di = 1.0 / (d11 * d22 - d21 * d21);
+  const double i00 = d22 * di, i01 = -d21 * di, i11 = d11 * di;
+  l0 = fma(a, i00, b * i01);
+  l1 = fma(a, i01, b * i11);
+}
 
 __device__ void phase_a_item(const DevState& s, const FactorParams& prm, BigFront* B, int chunk,
                              RowsSm& sm) {
@@ -710,14 +772,9 @@ __device__ void phase_a_item(const DevState& s, const FactorParams& prm, BigFron
     sm.sd[3 * tid + 2] = X[kXD + 3 * tid + 2];
     // 1x1 pivots scale their column by 1/d, as the reference does
     sm.sinv[tid] = (xi[kIKind + tid] == 1) ? 1.0 / X[kXD + 3 * tid] : 0.0;
-    const unsigned long long* below = reinterpret_cast<const unsigned long long*>(X + kXBelow);
-    sm.scm[tid] = fmax(X[kXCin + tid], __longlong_as_double((long long)below[tid]));
-    sm.srm[tid] = X[kXRin + tid];
   }
   __syncthreads();
-  if (tid == 0) sm.np = passing_prefix(sm, xi[kIAcc], prm.ustab, prm.pivot_tol);
-  __syncthreads();
-  const int np = sm.np;
+  const int np = xi[kINp];
   double* F = s.dpool + B->doff;
   const double* Wg = s.dpool + B->woff;
   // L of the accepted pivots on the rows below the block
@@ -728,11 +785,10 @@ __device__ void phase_a_item(const DevState& s, const FactorParams& prm, BigFron
         F[r + (size_t)f * (k + p)] = Wg[(size_t)p * f + r] * sm.sinv[p];
         p += 1;
       } else {
-        const double d11 = sm.sd[3 * p], d21 = sm.sd[3 * p + 1], d22 = sm.sd[3 * p + 2];
-        const double di = 1.0 / (d11 * d22 - d21 * d21);
-        const double a = Wg[(size_t)p * f + r], b = Wg[(size_t)(p + 1) * f + r];
-        F[r + (size_t)f * (k + p)] = a * (d22 * di) + b * (-d21 * di);
-        F[r + (size_t)f * (k + p + 1)] = a * (-d21 * di) + b * (d11 * di);
+        double l0, l1;
+        l_2x2(sm.sd + 3 * p, Wg[(size_t)p * f + r], Wg[(size_t)(p + 1) * f + r], l0, l1);
+        F[r + (size_t)f * (k + p)] = l0;
+        F[r + (size_t)f * (k + p + 1)] = l1;
         p += 2;
       }
     }
@@ -805,8 +861,6 @@ __device__ void phase_a_item(const DevState& s, const FactorParams& prm, BigFron
       atomicAdd(s.flops + 5, 1.0);
       if (np < acc) atomicAdd(s.flops + 6, 1.0);
       atomicAdd(s.flops + 7, (double)(nd - (np < acc ? 1 : 0)));
-      // the next panel's column maxima, filled by the trailing update
-      for (int j = 0; j < kBlk; j++) X[kXNext + j] = 0.0;
       B->state = (nd == 0 && k + np >= ncand) ? 1 : 0;
     }
   }
@@ -816,18 +870,27 @@ __device__ void phase_a_item(const DevState& s, const FactorParams& prm, BigFron
 // ---------------------------------------------------------------- phase U
 
 // One 64 x 64 lower tile of front B's trailing matrix at rows i0, columns
-// j0: the rank-kw update with the panel's L (columns kstart..kstart+kw of F)
-// and W (Wg), in FP64.
-__device__ void phase_u_tile(const DevState& s, const BigFront& B, int i0, int j0, UpdSm& sm) {
+// j0: the rank-kw update with the panel's L (columns ks..ks+kw) and W (Wg),
+// in FP64; k = ks + kw is the trailing matrix's first position. L is read
+// from the front's columns once committed, or (from_w) formed from W and
+// the panel's D as the commit forms it.
+__device__ void phase_u_tile(const DevState& s, const BigFront& B, int i0, int j0, int k, int kw,
+                             int ks, bool from_w, UpdSm& sm) {
   const int tid = threadIdx.x;
   const int tx = tid & 15;
   const int ty = tid >> 4;
   const int f = B.f;
-  const int k = B.k;
-  const int kw = B.kw;
-  const int ks = B.kstart;
   double* F = s.dpool + B.doff;
   const double* W = s.dpool + B.woff;
+  if (from_w && tid < kBlk) {
+    const double* X = s.dpool + B.xoff;
+    const int kd = reinterpret_cast<const int*>(X + kXInt)[kIKind + tid];
+    sm.ukind[tid] = kd;
+    sm.ud[3 * tid] = X[kXD + 3 * tid];
+    sm.ud[3 * tid + 1] = X[kXD + 3 * tid + 1];
+    sm.ud[3 * tid + 2] = X[kXD + 3 * tid + 2];
+    sm.usinv[tid] = (kd == 1) ? 1.0 / X[kXD + 3 * tid] : 0.0;
+  }
   double cur[4][4];
 #pragma unroll
   for (int b = 0; b < 4; b++) {
@@ -849,7 +912,8 @@ __device__ void phase_u_tile(const DevState& s, const BigFront& B, int i0, int j
       pa[q] = 0.0;
       pb[q] = 0.0;
       if (c < kw) {
-        if (i0 + rr < f) pa[q] = F[i0 + rr + (size_t)f * (ks + c)];
+        if (i0 + rr < f)
+          pa[q] = from_w ? W[(size_t)c * f + i0 + rr] : F[i0 + rr + (size_t)f * (ks + c)];
         if (j0 + rr < f) pb[q] = W[(size_t)c * f + j0 + rr];
       }
     }
@@ -865,6 +929,22 @@ __device__ void phase_u_tile(const DevState& s, const BigFront& B, int i0, int j
     }
   }
   __syncthreads();
+  if (from_w) {
+    // L = W D^-1 on the tile's rows, the commit's expressions
+    for (int e = tid; e < kw * kTileU; e += kThreads) {
+      const int c = e / kTileU, rr = e - c * kTileU;
+      const int kd = sm.ukind[c];
+      if (kd == 1) {
+        sm.As[c][rr] = sm.As[c][rr] * sm.usinv[c];
+      } else if (kd == 2) {
+        double l0, l1;
+        l_2x2(sm.ud + 3 * c, sm.As[c][rr], sm.As[c + 1][rr], l0, l1);
+        sm.As[c][rr] = l0;
+        sm.As[c + 1][rr] = l1;
+      }
+    }
+    __syncthreads();
+  }
   double acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; a++)
@@ -915,9 +995,13 @@ __device__ void phase_u_tile(const DevState& s, const BigFront& B, int i0, int j
   __syncthreads();
 }
 
-__device__ __forceinline__ long long tri_tiles(const BigFront& B, int tile) {
-  const long long t = (B.f - B.k + tile - 1) / tile;
+__device__ __forceinline__ long long tri_tiles_rows(int rows, int tile) {
+  const long long t = (rows + tile - 1) / tile;
   return t * (t + 1) / 2;
+}
+
+__device__ __forceinline__ long long tri_tiles(const BigFront& B, int tile) {
+  return tri_tiles_rows(B.f - B.k, tile);
 }
 
 __device__ __forceinline__ void tri_decode(long long lt, int& I, int& J) {
@@ -949,7 +1033,8 @@ __device__ int phase_u_tile_mixed(const DevState& s, const BigFront& B, int I, i
   for (int a = 0; a < 2; a++)
     for (int b = 0; b < 2; b++) {
       const int si = i0 + a * kTileU, sj = j0 + b * kTileU;
-      if (si < f && sj < f && si + kTileU - 1 >= sj) phase_u_tile(s, B, si, sj, sm);
+      if (si < f && sj < f && si + kTileU - 1 >= sj)
+        phase_u_tile(s, B, si, sj, B.k, B.kw, B.kstart, false, sm);
     }
   return 0;
 }
@@ -986,9 +1071,23 @@ __global__ void __launch_bounds__(kThreads, 1)
     {
       WarpDiag& w = reinterpret_cast<WarpDiag*>(dsm)[warp];
       if (blockIdx.x == 0 && tid == 0) counters[(step + 1) & 1] = 0;
-      for (int i = gwarp; i < nl; i += nwarp) {
-        const int on = phase_d_front(s, prm, s.big + list[i], step, w, done, meta);
-        if (on && (tid & 31) == 0) atomicAdd(counters + (step & 1), 1);
+      if (nl <= (int)gridDim.x) {
+        // a CTA per front: its threads apply the delays, warp 0 the block
+        if ((int)blockIdx.x < nl) {
+          BigFront* B = s.big + list[blockIdx.x];
+          if (phase_d_prepare<kThreads>(s, B, done, meta, tid) && warp == 0) {
+            phase_d_block(s, prm, B, step, w);
+            if (tid == 0) atomicAdd(counters + (step & 1), 1);
+          }
+        }
+      } else {
+        for (int i = gwarp; i < nl; i += nwarp) {
+          BigFront* B = s.big + list[i];
+          if (phase_d_prepare<32>(s, B, done, meta, tid & 31)) {
+            phase_d_block(s, prm, B, step, w);
+            if ((tid & 31) == 0) atomicAdd(counters + (step & 1), 1);
+          }
+        }
       }
     }
     grid.sync();
@@ -1003,11 +1102,47 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int fi = item_front(P, n, t);
         const BigFront& B = s.big[list[c0 + fi]];
         const int nchunk = (int)(P.ptr[fi + 1] - P.ptr[fi]);
-        phase_r_item(s, B, (int)(t - P.ptr[fi]), nchunk, sm);
+        phase_r_item(s, prm, B, (int)(t - P.ptr[fi]), nchunk, sm);
       }
       __syncthreads();
     }
     grid.sync();
+    if (!prm.mixed) {
+      // ---- A and U together: the row chunks that write L and commit the
+      // panel, then the trailing-update tiles, which form L from W and take
+      // the panel's position from the scratch, not from the descriptor that
+      // the commit changes meanwhile
+      for (int c0 = 0; c0 < nl; c0 += kChunkFronts) {
+        const int n = min(kChunkFronts, nl - c0);
+        const long long total = front_prefix(P, n, [&](int i) {
+          const BigFront& B = s.big[list[c0 + i]];
+          const int ra = row_chunks(s, B, step);
+          if (ra == 0) return 0ll;
+          const int* xi = xint(s.dpool + B.xoff);
+          const int np = xi[kINp];
+          return (long long)ra + (np > 0 ? tri_tiles_rows(B.f - (xi[kIK] + np), kTileU) : 0ll);
+        });
+        for (long long t = blockIdx.x; t < total; t += gridDim.x) {
+          const int fi = item_front(P, n, t);
+          BigFront* B = s.big + list[c0 + fi];
+          const long long it = t - P.ptr[fi];
+          const int ra = row_chunks(s, *B, step);
+          if (it < ra) {
+            phase_a_item(s, prm, B, (int)it, *reinterpret_cast<RowsSm*>(dsm));
+          } else {
+            const int* xi = xint(s.dpool + B->xoff);
+            const int ks = xi[kIK], np = xi[kINp];
+            int I, J;
+            tri_decode(it - ra, I, J);
+            phase_u_tile(s, *B, ks + np + I * kTileU, ks + np + J * kTileU, ks + np, np, ks, true,
+                         *reinterpret_cast<UpdSm*>(dsm));
+          }
+        }
+        __syncthreads();
+      }
+      grid.sync();
+      continue;
+    }
     // ---- A: the same items; the first one of a front commits the panel
     for (int c0 = 0; c0 < nl; c0 += kChunkFronts) {
       const int n = min(kChunkFronts, nl - c0);
@@ -1021,13 +1156,13 @@ __global__ void __launch_bounds__(kThreads, 1)
       __syncthreads();
     }
     grid.sync();
-    // ---- U: trailing-update tiles of the fronts that accepted pivots
-    const int tile = prm.mixed ? umma::kTileM : kTileU;
+    // ---- U (mixed precision): trailing-update tiles of the fronts that
+    // accepted pivots, after the commit
     for (int c0 = 0; c0 < nl; c0 += kChunkFronts) {
       const int n = min(kChunkFronts, nl - c0);
       const long long total = front_prefix(P, n, [&](int i) {
         const BigFront& B = s.big[list[c0 + i]];
-        return (active(s, B, step) && B.kw > 0) ? tri_tiles(B, tile) : 0ll;
+        return (active(s, B, step) && B.kw > 0) ? tri_tiles(B, umma::kTileM) : 0ll;
       });
       UpdSm& sm = *reinterpret_cast<UpdSm*>(dsm);
       for (long long t = blockIdx.x; t < total; t += gridDim.x) {
@@ -1035,9 +1170,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const BigFront& B = s.big[list[c0 + fi]];
         int I, J;
         tri_decode(t - P.ptr[fi], I, J);
-        if (!prm.mixed) {
-          phase_u_tile(s, B, B.k + I * kTileU, B.k + J * kTileU, sm);
-        } else if (!tc_fail) {
+        if (!tc_fail) {
           // the tensor-core operands share the dynamic shared memory with
           // the FP64 tiles' panels (a tile uses one or the other)
           float* ops = reinterpret_cast<float*>(dsm + kOpsOffset);
