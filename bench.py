@@ -360,23 +360,35 @@ def run_ours(args, world, rank, local):
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         return float(t.item())
 
-    # (1) the reference's pivot order: every factorization starts from the
-    # symbolic supernodes and replays the reference's delays
-    for _ in range(args.warmup):
-        step()
-    ms_ref_order = timed(args.steps)
-    berr_ref_order = backward_error(s, x.cpu().numpy(), s.rhs)
-    delayed_ref_order = ldl.stats()["delayed"]
+    ref_order = same_values = None
+    if not args.headline_only:
+        # (1) the reference's pivot order: every factorization starts from
+        # the symbolic supernodes and replays the reference's delays
+        for _ in range(args.warmup):
+            step()
+        ms_ref_order = timed(args.steps)
+        ref_order = {
+            "value": world * args.steps / (ms_ref_order / 1e3),
+            "ms_per_step": ms_ref_order / args.steps,
+            "backward_error": backward_error(s, x.cpu().numpy(), s.rhs),
+            "delayed_pivots": ldl.stats()["delayed"],
+            "what": "every factorization from the symbolic supernodes, the reference's "
+                    "pivot sequence replayed (the first factorization of a pattern)"}
 
-    # (2) the record of a factorization of these very values: the fastest
-    # case of pivot-order reuse (every recorded pivot passes again)
-    ldl.factor(dvec)
-    ldl.reuse_pivot_order()
-    for _ in range(args.warmup):
-        step()
-    ms_same = timed(args.steps)
-    berr_same = backward_error(s, x.cpu().numpy(), s.rhs)
-    delayed_same = ldl.stats()["delayed"]
+        # (2) the record of a factorization of these very values: the
+        # fastest case of pivot-order reuse (every recorded pivot passes)
+        ldl.factor(dvec)
+        ldl.reuse_pivot_order()
+        for _ in range(args.warmup):
+            step()
+        ms_same = timed(args.steps)
+        same_values = {
+            "value": world * args.steps / (ms_same / 1e3),
+            "ms_per_step": ms_same / args.steps,
+            "backward_error": backward_error(s, x.cpu().numpy(), s.rhs),
+            "delayed_pivots": ldl.stats()["delayed"],
+            "what": "record taken from a factorization of the benchmark matrix itself (the "
+                    "best case of reuse, e.g. inertia-correction refactorizations)"}
 
     # (3) the headline: the pivot order recorded at a neighbouring
     # interior-point iterate (the same pattern, other values), as a
@@ -544,7 +556,11 @@ def run_ours(args, world, rank, local):
                             "peak (37 TFLOP/s, not measured here)"}
         roof.update({"kernel": dom["name"], "launches": dom["launches"],
                      "ms_per_launch": per_launch_ms, "peak_source": peaks["source"],
-                     "traffic_note": "DRAM bytes per launch from ncu are in profiles/",
+                     "traffic_note": "null: the dominant class is one cooperative launch per "
+                                     "tree level; its full ncu capture (128x128, "
+                                     "profiles/app_level_kernel_plane_stress_128.txt) is "
+                                     "L2-resident, 6.7 MB DRAM read per level launch, so no "
+                                     "full-size DRAM figure is scaled from it",
                      "timing": "profile pass of the same steps, CUDA events per kernel class"})
 
     cpu = None
@@ -575,18 +591,8 @@ def run_ours(args, world, rank, local):
                            "delayed when it fails",
             "l2": "inputs and per-step factor traffic larger than L2 (126 MB); no flush",
         },
-        "fp64_reference_order": {
-            "value": world * args.steps / (ms_ref_order / 1e3),
-            "ms_per_step": ms_ref_order / args.steps, "backward_error": berr_ref_order,
-            "delayed_pivots": delayed_ref_order,
-            "what": "every factorization from the symbolic supernodes, the reference's "
-                    "pivot sequence replayed (the first factorization of a pattern)"},
-        "pivot_record_from_same_values": {
-            "value": world * args.steps / (ms_same / 1e3),
-            "ms_per_step": ms_same / args.steps, "backward_error": berr_same,
-            "delayed_pivots": delayed_same,
-            "what": "record taken from a factorization of the benchmark matrix itself (the "
-                    "best case of reuse, e.g. inertia-correction refactorizations)"},
+        "fp64_reference_order": ref_order,
+        "pivot_record_from_same_values": same_values,
         "mixed_precision": mixed,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "backward_error": berr_e2e},
@@ -735,6 +741,9 @@ def main(argv=None) -> int:
     ap.add_argument("--no-profile-pass", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-clocks", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-mixed", action="store_true", help=argparse.SUPPRESS)
+    # profiling runs: only the headline's pivot order (no reference-order and
+    # same-values arms)
+    ap.add_argument("--headline-only", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--workload", choices=["plane_stress", "batched"], default="plane_stress",
                     help=argparse.SUPPRESS)
     ap.add_argument("--systems", type=int, default=512, help=argparse.SUPPRESS)
