@@ -21,7 +21,7 @@ from __future__ import annotations
 
 import torch
 
-from .sparse_ldl import SparseLDL, Vector
+from .sparse_ldl import SparseLDL, SparseLDLBatch, Vector
 
 __all__ = ["kkt_solve"]
 
@@ -31,9 +31,14 @@ class _KKTSolve(torch.autograd.Function):
     def forward(ctx, vals, diag, b, ldl):
         if not (vals.is_cuda and b.is_cuda):
             raise TypeError("kkt_solve needs CUDA tensors")
-        ldl.mat.vals = vals.detach().contiguous().to(torch.float64)
+        v = vals.detach().contiguous().to(torch.float64)
         d = None if diag is None else diag.detach().contiguous().to(torch.float64)
-        ldl.factor(Vector(d) if d is not None else None)
+        dv = Vector(d) if d is not None else None
+        if isinstance(ldl, SparseLDLBatch):
+            ldl.factor(dv, values=v)
+        else:
+            ldl.mat.vals = v
+            ldl.factor(dv)
         x = b.detach().to(torch.float64).clone()
         if x.dim() == 2:
             x = x.t().contiguous().t()
@@ -58,7 +63,9 @@ class _KKTSolve(torch.autograd.Function):
 def kkt_solve(ldl: SparseLDL, vals: torch.Tensor, diag: torch.Tensor | None,
               b: torch.Tensor) -> torch.Tensor:
     """x = K^{-1} b with K = CSR(vals) + diag(diag) on ``ldl``'s pattern;
-    differentiable in vals, diag and b. The factor is stored in ``ldl`` and
+    differentiable in vals, diag and b. ``ldl`` may be a SparseLDLBatch:
+    vals, diag and b are then the systems' arrays concatenated, and K is
+    block diagonal. The factor is stored in ``ldl`` and
     reused by the backward pass, so call backward before refactoring
     ``ldl``."""
     return _KKTSolve.apply(vals, diag, b, ldl)

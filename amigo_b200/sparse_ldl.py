@@ -603,10 +603,11 @@ class SparseLDLBatch(SparseLDL):
         return np.concatenate([np.asarray(v.cpu().numpy() if _is_torch(v) else v, np.float64)
                                for v in vals])
 
-    def factor(self, diagonal=None) -> int:
-        """Factor every system with its current values; ``diagonal`` is the
+    def factor(self, diagonal=None, values=None) -> int:
+        """Factor every system with its current values, or with ``values``
+        (the systems' values concatenated) when given; ``diagonal`` is the
         concatenated diagonal vector (or a list of per-system vectors)."""
-        self.mat.vals = self._gather_values()
+        self.mat.vals = self._gather_values() if values is None else values
         if isinstance(diagonal, (list, tuple)):
             parts = [_values_of(d) for d in diagonal]
             if any(_is_torch(d) for d in parts):
