@@ -354,13 +354,42 @@ __device__ int phase_d_prepare(const DevState& s, BigFront* B, int* done, int* m
           t = orig[a];
           orig[a] = orig[b];
           orig[b] = t;
-          // columns that moved lose their estimate
-          if (a - k < kBlk) X[kXNext + (a - k)] = 0.0;
-          if (b - k < kBlk) X[kXNext + (b - k)] = 0.0;
         }
       }
       ncand--;
       group_sync<NT>();
+    }
+    // The next panel's first test needs the exact maximum below the block
+    // of the column it tests. The interchanges exchanged rows inside the
+    // block's positions with rows below them, so the maxima are formed
+    // again from the columns (rows from k + kBlk on, contiguous in the lower
+    // triangle): every position of the block when a CTA applies the delays,
+    // the positions that received another candidate when a warp does.
+    if constexpr (NT > 32) {
+      const int lane = g & 31, wq = g >> 5;
+      for (int c = k + wq; c < k + kBlk && c < f; c += NT / 32) {
+        const double* col = F + (size_t)f * c;
+        double m = 0.0;
+        for (int i = k + kBlk + lane; i < f; i += 32) m = fmax(m, fabs(col[i]));
+        m = warp_max(m);
+        if (lane == 0) X[kXNext + (c - k)] = m;
+      }
+      group_sync<NT>();
+    } else {
+      for (int q = 0; q < nd; q++) {
+        const int a = xi[kIDpos + q];
+        const int b = B->ncand - 1 - q;
+        for (int h = 0; h < 2; h++) {
+          const int c = h ? b : a;
+          if (c - k >= kBlk || (h && b <= a)) continue;
+          const double* col = F + (size_t)f * c;
+          double m = 0.0;
+          for (int i = k + kBlk + g; i < f; i += NT) m = fmax(m, fabs(col[i]));
+          m = warp_max(m);
+          if (g == 0) X[kXNext + (c - k)] = m;
+          group_sync<NT>();
+        }
+      }
     }
     if (g == 0) {
       B->ncand = ncand;
