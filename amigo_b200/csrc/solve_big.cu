@@ -67,7 +67,7 @@ __device__ __forceinline__ bool is_second(const unsigned* secw, int p) {
   return (secw[p >> 5] >> (p & 31)) & 1u;
 }
 
-__global__ void __launch_bounds__(kSbThreads)
+__global__ void __launch_bounds__(kSbThreads, 1)
     forward_big_kernel(DevPlan p, DevState s, const int* __restrict__ nodes,
                        double* __restrict__ x, int ldx, int nrhs, int r0rhs, int nr,
                        double* __restrict__ upool) {
@@ -111,7 +111,10 @@ __global__ void __launch_bounds__(kSbThreads)
     for (int r = 0; r < nr; r++) dst[(size_t)r * R] = x[(size_t)ldx * (r0rhs + r) + var];
   }
   cl.sync();
-  // children's update vectors, one child at a time (fixed summation order)
+  // children's update vectors, one child at a time (fixed summation order).
+  // Every CTA reads each child's entries and adds the ones that land in its
+  // own rows, so no two CTAs write a row and a CTA barrier separates the
+  // children
   {
     const int kb = p.kid_ptr[node];
     const int ke = p.kid_ptr[node + 1];
@@ -122,7 +125,8 @@ __global__ void __launch_bounds__(kSbThreads)
       const int mc = s.f[ch] - s.npiv[ch];
       const double* uc = upool + s.u_off[ch] * nrhs + (size_t)r0rhs * mc;
       const int* cm = p.cmap + p.cptr[ch];
-      for (int t = gt; t < mc; t += kSbCL * kSbThreads) {
+#pragma unroll 1
+      for (int t = tid; t < mc; t += kSbThreads) {
         int q;
         if (t < nd) {
           q = off + t;
@@ -131,17 +135,32 @@ __global__ void __launch_bounds__(kSbThreads)
           if (q >= ns) q += nd_in;
         }
         q = post_of[q];
-        const int o = q / R;
-        double* dst = at_rank(cl, v, o, rank) + (q - o * R);
-        for (int r = 0; r < nr; r++) dst[(size_t)r * R] += uc[(size_t)r * mc + t];
+        if (q / R == rank) {
+          double* dst = v + (q - rank * R);
+#pragma unroll 1
+          for (int r = 0; r < nr; r++) dst[(size_t)r * R] += uc[(size_t)r * mc + t];
+        }
       }
-      cl.sync();
+      __syncthreads();
       off += nd;
     }
   }
 
   // unit-lower solve, tile by tile
   const int ntile = (npiv + kTileR - 1) / kTileR;
+  // a tile's entries of this thread's first row below it: loaded a tile
+  // ahead (they do not depend on the solved values), so that their HBM
+  // latency overlaps the previous tile's update, barrier and solve
+  double lvn[kTileR];
+  auto prefetch = [&](int tb_) {
+    const int jb_ = tb_ * kTileR;
+    const int nb_ = min(jb_ + kTileR, npiv) - jb_;
+    const int i_ = max(jb_ + nb_, rb) + tid;
+    const double* li_ = L + i_ + (size_t)ldl * jb_;
+#pragma unroll
+    for (int j = 0; j < kTileR; j++) lvn[j] = (i_ < re && j < nb_) ? li_[(size_t)ldl * j] : 0.0;
+  };
+  if (ntile > 0) prefetch(0);
   for (int b = 0; b < ntile; b++) {
     const int jb = b * kTileR;
     const int je = min(jb + kTileR, npiv);
@@ -189,16 +208,22 @@ __global__ void __launch_bounds__(kSbThreads)
     __syncthreads();
     // a 2x2 pair across the tile boundary: its D slot (je, je - 1) is skipped
     const int skip_i = (je < npiv && is_second(secw, je)) ? je : -1;
+    double lv0[kTileR];
+#pragma unroll
+    for (int j = 0; j < kTileR; j++) lv0[j] = lvn[j];
+    if (b + 1 < ntile) prefetch(b + 1);
     for (int i = max(je, rb) + tid; i < re; i += kSbThreads) {
       double acc[kSbRhs];
 #pragma unroll
       for (int r = 0; r < kSbRhs; r++) acc[r] = 0.0;
       const double* li = L + i + (size_t)ldl * jb;
       // the row's tile entries are all loaded before the products, so that
-      // their HBM latency is paid once per row, not once per column
+      // their HBM latency is paid once per row, not once per column (the
+      // first row's were loaded a tile ahead)
+      const bool first = i < max(je, rb) + kSbThreads;
       double lv[kTileR];
 #pragma unroll
-      for (int j = 0; j < kTileR; j++) lv[j] = (j < nb) ? li[(size_t)ldl * j] : 0.0;
+      for (int j = 0; j < kTileR; j++) lv[j] = first ? lv0[j] : (j < nb) ? li[(size_t)ldl * j] : 0.0;
 #pragma unroll
       for (int j = 0; j < kTileR; j++) {
         const double l = (i == skip_i && j == nb - 1) ? 0.0 : lv[j];
