@@ -26,6 +26,7 @@ SIGNATURES = {
     "b200ldl_set_stream": (ctypes.c_int, [_vp, _vp]),
     "b200ldl_factor": (ctypes.c_int, [_vp, _vp, _vp]),
     "b200ldl_factor_host": (ctypes.c_int, [_vp, _f64p, _f64p]),
+    "b200ldl_factor_elements": (ctypes.c_int, [_vp, _vp, _vp, _vp]),
     "b200ldl_solve": (ctypes.c_int, [_vp, ctypes.c_int, _vp, ctypes.c_int]),
     "b200ldl_solve_host": (ctypes.c_int, [_vp, ctypes.c_int, _f64p, ctypes.c_int]),
     "b200ldl_solve_refine": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp,

@@ -90,6 +90,11 @@ struct b200ldl_handle {
   double refine_tol = 1e-12;
   bool factored_mixed = false;
   const double* last_vals = nullptr;
+  // element-block source of the factorization in progress (nullptr: CSR
+  // values)
+  const long long* asm_ptr = nullptr;
+  const long long* asm_src = nullptr;
+  const double* asm_blocks = nullptr;
   const double* last_diag = nullptr;
   int last_iters = 0;
   double last_berr = 0.0;
@@ -484,6 +489,9 @@ void bind_state(b200ldl_t h) {
   st.class_list = h->d_class_list.ptr;
   for (int c = 0; c < 5; c++) st.cf_limit[c] = cluster_front_limit(c);
   st.partner = h->replanned ? h->d_partner.ptr : nullptr;
+  st.asm_ptr = h->asm_ptr;
+  st.asm_src = h->asm_src;
+  st.asm_blocks = h->asm_blocks;
 }
 
 void ensure_pools(b200ldl_t h) {
@@ -927,6 +935,42 @@ int b200ldl_factor(b200ldl_t h, const double* vals, const double* diag) {
     h->factored = false;
     h->fmax = 0;
     run_factor(h, vals, diag);
+    return 0;
+  });
+}
+
+int b200ldl_factor_elements(b200ldl_t h, b200ldl_assembly_t a, const double* blocks,
+                            const double* diag) {
+  return guarded(h, [&]() {
+    int an = 0, annz = 0;
+    const long long *aptr = nullptr, *asrc = nullptr;
+    if (!a || assembly_device_plan(a, &an, &annz, &aptr, &asrc) != 0)
+      return fail(h, -1, "no assembly plan");
+    if (an != h->n || annz != h->nnz)
+      return fail(h, -1,
+                  "the assembly plan is for another pattern (n %d nnz %d, handle n %d nnz %d)",
+                  an, annz, h->n, h->nnz);
+    if (h->nnz > 0 && !blocks) return fail(h, -1, "blocks is null");
+    if (h->precision != B200LDL_FP64)
+      return fail(h, -1,
+                  "element-block factorization needs the FP64 mode (the mixed mode refines "
+                  "against CSR values)");
+    // the source holds for this factorization only, whatever happens in it
+    struct Source {
+      b200ldl_t h;
+      ~Source() {
+        h->asm_ptr = h->asm_src = nullptr;
+        h->asm_blocks = nullptr;
+        h->st.asm_ptr = h->st.asm_src = nullptr;
+        h->st.asm_blocks = nullptr;
+      }
+    } source{h};
+    h->asm_ptr = h->st.asm_ptr = aptr;
+    h->asm_src = h->st.asm_src = asrc;
+    h->asm_blocks = h->st.asm_blocks = blocks;
+    h->factored = false;
+    h->fmax = 0;
+    run_factor(h, nullptr, diag);
     return 0;
   });
 }

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "../../include/b200ldl.h"
+#include "ldl_internal.h"
 
 namespace {
 
@@ -201,3 +202,17 @@ const char* b200ldl_assembly_last_error(b200ldl_assembly_t a) {
 void b200ldl_assembly_destroy(b200ldl_assembly_t a) { delete a; }
 
 }  // extern "C"
+
+namespace b200ldl {
+
+int assembly_device_plan(const ::b200ldl_assembly* a, int* n, int* nnz, const long long** ptr,
+                         const long long** src) {
+  if (!a || !a->d_ptr.ptr) return -1;
+  *n = a->n;
+  *nnz = a->nnz;
+  *ptr = a->d_ptr.ptr;
+  *src = a->d_src.ptr;
+  return 0;
+}
+
+}  // namespace b200ldl

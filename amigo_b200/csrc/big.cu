@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(256) big_assemble_kernel(DevPlan p, DevState s
          e += (int64_t)CL * blockDim.x) {
       int r = p.scat_row[e];
       if (r >= ns) r += nd_in;
-      F[r + (size_t)f * p.scat_col[e]] += vals[p.scat_csr[e]];
+      F[r + (size_t)f * p.scat_col[e]] += csr_value(s, vals, p.scat_csr[e]);
     }
   }
   // the children's contribution blocks, one child after another

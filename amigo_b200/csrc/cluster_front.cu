@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(kCfThreads)
       int r = p.scat_row[e];
       if (r >= ns) r += nd_in;
       double* dst = row_ptr<CL>(cl, tri, rank, r) + p.scat_col[e];
-      *dst += vals[p.scat_csr[e]];
+      *dst += csr_value(s, vals, p.scat_csr[e]);
     }
   }
   csync<CL>(cl);

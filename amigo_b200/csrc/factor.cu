@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(kFactorThreads)
     for (int64_t e = e0 + tid; e < e1; e += blockDim.x) {
       int r = p.scat_row[e];
       if (r >= ns) r += nd_in;
-      F[r + (size_t)ld * p.scat_col[e]] += vals[p.scat_csr[e]];
+      F[r + (size_t)ld * p.scat_col[e]] += csr_value(s, vals, p.scat_csr[e]);
     }
   }
   __syncthreads();

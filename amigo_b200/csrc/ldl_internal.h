@@ -7,6 +7,8 @@
 #include <utility>
 #include <vector>
 
+struct b200ldl_assembly;  // the assembly plan of the C ABI (assembly.cu)
+
 namespace b200ldl {
 
 // Work counters accumulated on the device per factorization.
@@ -166,7 +168,26 @@ struct DevState {
   // formed a 2x2 pivot with v in the record, -1 otherwise (nullptr without a
   // record)
   const int* partner;
+  // factorization from element Hessian blocks (b200ldl_factor_elements): the
+  // CSR value of entry e is the sum, from zero in order, of
+  // asm_blocks[asm_src[q]] for q in [asm_ptr[e], asm_ptr[e + 1]); nullptr
+  // when the factorization reads CSR values
+  const long long* asm_ptr;
+  const long long* asm_src;
+  const double* asm_blocks;
 };
+
+// The CSR value of entry e: from the values, or assembled from the element
+// blocks in the order of the assembly kernel (assembly.cu), so that a front
+// receives the same bits either way.
+__device__ __forceinline__ double csr_value(const DevState& s, const double* __restrict__ vals,
+                                            long long e) {
+  if (!s.asm_blocks) return vals[e];
+  double v = 0.0;
+  const long long q1 = s.asm_ptr[e + 1];
+  for (long long q = s.asm_ptr[e]; q < q1; q++) v += s.asm_blocks[s.asm_src[q]];
+  return v;
+}
 
 struct FactorParams {
   double ustab;
@@ -287,5 +308,10 @@ void launch_copy_cols(int n, int nr, const double* src, int lds, double* dst, in
 // (+dx), bit 1 = constraint row (-dc)
 void launch_perturb_diag(int n, const double* diag, const unsigned char* cls, double dx,
                          double dc, double* out, cudaStream_t st);
+
+// The device copy of an assembly plan (assembly.cu): its pattern's size and
+// the per-CSR-entry contribution lists. Returns 0, or -1 without a plan.
+int assembly_device_plan(const ::b200ldl_assembly* a, int* n, int* nnz, const long long** ptr,
+                         const long long** src);
 
 }  // namespace b200ldl

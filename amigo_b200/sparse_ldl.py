@@ -188,6 +188,34 @@ class SparseLDL:
             d.ctypes.data_as(_native._f64p) if d is not None else None)
         return _native.check(self._h, st, "factor")
 
+    def factor_elements(self, assembly, blocks, diagonal=None) -> int:
+        """Factor from the element Hessian blocks through ``assembly`` (an
+        amigo_b200.assembly.CSRAssembly of this pattern) without forming the
+        CSR values: each front reads its entries as sums of their element
+        contributions, in the order CSRAssembly.values sums them, so the
+        factorization is the one of ``factor`` after ``values``. ``blocks``
+        as CSRAssembly.values takes them; CUDA tensors."""
+        import torch
+
+        if isinstance(blocks, (list, tuple)):
+            blocks = torch.cat([b.reshape(-1) for b in blocks])
+        if not (torch.is_tensor(blocks) and blocks.is_cuda and blocks.dtype == torch.float64):
+            raise TypeError("blocks must be a float64 CUDA tensor")
+        blocks = blocks.contiguous().reshape(-1)
+        if blocks.numel() != assembly.nvals:
+            raise ValueError(f"expected {assembly.nvals} block values, got {blocks.numel()}")
+        diag = _values_of(diagonal)
+        if diag is not None:
+            if not _is_torch(diag):
+                diag = torch.as_tensor(np.asarray(diag, np.float64), device=blocks.device)
+            diag = diag.contiguous().to(device=blocks.device, dtype=torch.float64)
+        self._keep = [blocks, diag]
+        self._sync_stream(blocks)
+        st = self._lib.b200ldl_factor_elements(
+            self._h, assembly._h, ctypes.c_void_p(blocks.data_ptr()),
+            ctypes.c_void_p(diag.data_ptr()) if diag is not None else None)
+        return _native.check(self._h, st, "factor_elements")
+
     def _sync_stream(self, t):
         import torch
 

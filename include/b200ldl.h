@@ -322,6 +322,24 @@ int b200ldl_assembly_plan(b200ldl_assembly_t a, long long* ptr, long long* src);
 const char* b200ldl_assembly_last_error(b200ldl_assembly_t a);
 void b200ldl_assembly_destroy(b200ldl_assembly_t a);
 
+/* Factor from element Hessian blocks without forming the CSR values: the
+ * front assembly of b200ldl_factor reads each CSR entry as the sum of its
+ * element contributions through the assembly plan a (built by
+ * b200ldl_assembly_create for this handle's pattern), in the plan's order,
+ * so every front receives the same bits as from b200ldl_assembly_values
+ * followed by b200ldl_factor. blocks (the element blocks as
+ * b200ldl_assembly_values takes them) and diag: DEVICE pointers. Replaces
+ * the reference's assembly into a CSR matrix followed by the factorization:
+ * ComponentGroup::add_hessian_kernel + CSRMat::add_row
+ * (include/component_group.h:144-162, include/csr_matrix.h:554-567) or the
+ * GPU hessian_kernel_atomic (include/cuda/component_group_backend.cuh:
+ * 157-190), then SparseLDL::factor(diag) (include/sparse_ldl.h:136-158).
+ * FP64 mode only (status -1 in the mixed mode, whose refinement needs the
+ * CSR values); the solves work as after b200ldl_factor, b200ldl_solve_refine
+ * excepted (it needs the values). */
+int b200ldl_factor_elements(b200ldl_t h, b200ldl_assembly_t a, const double* blocks,
+                            const double* diag);
+
 /* Dense Schur-complement update on the Blackwell tensor cores (no
  * counterpart in the reference, whose frontal_trailing_update,
  * include/sparse_ldl.h:1190-1215, calls FP64 dgemm): C -= A B^T for A (m x
