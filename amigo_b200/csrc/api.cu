@@ -122,6 +122,10 @@ struct b200ldl_handle {
   // a level whose fronts cannot exceed the shared-memory limit, whatever the
   // delays, needs no big-front launch (and no host read-back)
   std::vector<char> level_may_big;
+  std::vector<int> level_fbound;  // per level: bound on its on-chip fronts (shared memory sizing)
+  // per level: the on-chip front size its small-front launch is given, the
+  // last factorization's largest front plus slack (the bound until then)
+  std::vector<int> level_fcap;
   std::vector<int> h_ns, h_nc;
 
   // device plan
@@ -290,8 +294,16 @@ void build_plan(b200ldl_t h, const int* rowp, const int* cols) {
       fsb[k] = b;
     }
     h->level_may_big.assign(nl, 0);
-    for (int k = 0; k < nn; k++)
-      if (fsb[k] + nc[k] > kSmemFrontMax) h->level_may_big[level[k]] = 1;
+    h->level_fbound.assign(nl, 1);
+    for (int k = 0; k < nn; k++) {
+      const long long fb = fsb[k] + nc[k];
+      if (fb > kSmemFrontMax) h->level_may_big[level[k]] = 1;
+      // the on-chip front of the level's small-front launch: sized for its
+      // largest bound, so that small fronts leave room for more CTAs per SM
+      h->level_fbound[level[k]] =
+          std::max(h->level_fbound[level[k]], (int)std::min<long long>(fb, kSmemFrontMax));
+    }
+    h->level_fcap = h->level_fbound;
   }
   h->h_ns = ns;
   h->h_nc = nc;
@@ -520,6 +532,8 @@ void configure_device_kernels() {
   done[dev] = 1;
 }
 
+void level_fronts(b200ldl_t h);
+
 void run_factor_once(b200ldl_t h, const double* vals, const double* diag, bool mixed) {
   configure_device_kernels();
   // fronts re-planned from a pivot record are expected to accept their
@@ -546,8 +560,8 @@ void run_factor_once(b200ldl_t h, const double* vals, const double* diag, bool m
       if (h->level_may_big[l])
         CK(cudaMemsetAsync(h->d_big_meta.ptr, 0, kBigMeta * sizeof(int), h->stream));
       h->prof.begin(h->stream);
-      launch_factor_level(h->plan, h->st, h->d_level_nodes.ptr + b, cnt, prm, h->stream,
-                          vals, diag);
+      launch_factor_level(h->plan, h->st, h->d_level_nodes.ptr + b, cnt, h->level_fcap[l], prm,
+                          h->stream, vals, diag);
       h->prof.end(kPhFront, h->stream, 1);
       CK(cudaGetLastError());
       if (!h->level_may_big[l]) continue;
@@ -603,12 +617,27 @@ void run_factor_once(b200ldl_t h, const double* vals, const double* diag, bool m
         CK(cudaStreamSynchronize(h->stream));
       }
       h->factored = true;
+      // on-chip sizes for the next factorization: this one's largest front
+      // per level, with room for a quarter more (at least 8 rows) of delays
+      level_fronts(h);
+      for (int l = 0; l < h->num_levels; l++) {
+        const int fm = h->level_fmax[l];
+        h->level_fcap[l] = std::min(h->level_fbound[l],
+                                    std::min(kSmemFrontMax, fm + std::max(8, fm / 4)));
+      }
       return;
     }
-    // a pool ran out: grow both (the counters stop being meaningful after
-    // the first failure, so grow geometrically) and factor again
-    h->icap = std::max<unsigned long long>(h->icap * 2, h->used[0] + (1u << 16));
-    h->dcap = std::max<unsigned long long>(h->dcap * 2, h->used[1] + (1u << 20));
+    if (err[0] & 2) {
+      // a front outgrew its launch's on-chip size: every level gets its
+      // bound, which no front can exceed
+      h->level_fcap = h->level_fbound;
+    }
+    if (err[0] & 1) {
+      // a pool ran out: grow both (the counters stop being meaningful after
+      // the first failure, so grow geometrically) and factor again
+      h->icap = std::max<unsigned long long>(h->icap * 2, h->used[0] + (1u << 16));
+      h->dcap = std::max<unsigned long long>(h->dcap * 2, h->used[1] + (1u << 20));
+    }
   }
   throw std::runtime_error("factor storage did not converge after repeated growth");
 }

@@ -121,7 +121,7 @@ enum : int { kDelay = 0, kOne = 1, kTwo = 2, kNeedRow = 3, kZero = 4 };
 __global__ void __launch_bounds__(kFactorThreads)
     factor_level_kernel(DevPlan p, DevState s, const int* __restrict__ nodes,
                         const double* __restrict__ vals, const double* __restrict__ diag,
-                        FactorParams prm) {
+                        FactorParams prm, int fcap) {
   extern __shared__ __align__(16) double smem[];
   __shared__ Reduce red;
   __shared__ int sh_fail;
@@ -147,6 +147,17 @@ __global__ void __launch_bounds__(kFactorThreads)
   const bool big = f > kSmemFrontMax;
 
   if (tid == 0) {
+    // the launch's shared memory holds fronts up to fcap: a larger one stops
+    // the factorization, which the host repeats with room for every front
+    if (!big && f > fcap) {
+      atomicOr(s.err, 2);
+      atomicCAS(s.err + 1, -1, node);
+      sh_fail = 1;
+    }
+  }
+  __syncthreads();
+  if (sh_fail) return;
+  if (tid == 0) {
     int fail = 0;
     const unsigned long long io = atomicAdd(s.used, 2ull * (unsigned long long)f);
     if (io + 2ull * f > s.icap) fail = 1;
@@ -169,7 +180,7 @@ __global__ void __launch_bounds__(kFactorThreads)
       sh_doff = (long long)dofs;
     }
     if (fail) {
-      atomicExch(s.err, 1);
+      atomicOr(s.err, 1);  // a pool ran out
       atomicCAS(s.err + 1, -1, node);
     }
     sh_fail = fail;
@@ -611,7 +622,7 @@ __global__ void __launch_bounds__(kFactorThreads)
       sh_doff = (long long)dofs;
     }
     if (fail) {
-      atomicExch(s.err, 1);
+      atomicOr(s.err, 1);  // a pool ran out
       atomicCAS(s.err + 1, -1, node);
     }
     sh_fail = fail;
@@ -656,24 +667,23 @@ __global__ void __launch_bounds__(kFactorThreads)
 
 }  // namespace
 
-size_t factor_smem_bytes() {
-  // front (ld = f|1) plus two saved columns
-  const int f = kSmemFrontMax;
+size_t factor_smem_bytes(int f) {
+  // the front (ld = f|1) and two columns of slack
   return ((size_t)(f | 1) * f + 2 * (size_t)f) * sizeof(double);
 }
 
 void launch_factor_level(const DevPlan& p, const DevState& s, const int* level_nodes,
-                         int count, const FactorParams& prm, cudaStream_t stream,
+                         int count, int fmax, const FactorParams& prm, cudaStream_t stream,
                          const double* vals, const double* diag) {
   if (count <= 0) return;
-  factor_level_kernel<<<count, kFactorThreads, factor_smem_bytes(), stream>>>(
-      p, s, level_nodes, vals, diag, prm);
+  factor_level_kernel<<<count, kFactorThreads, factor_smem_bytes(fmax), stream>>>(
+      p, s, level_nodes, vals, diag, prm, fmax);
 }
 
 cudaError_t configure_factor_kernels() {
   return cudaFuncSetAttribute(factor_level_kernel,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)factor_smem_bytes());
+                              (int)factor_smem_bytes(kSmemFrontMax));
 }
 
 }  // namespace b200ldl

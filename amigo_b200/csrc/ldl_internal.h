@@ -146,7 +146,8 @@ struct DevState {
   unsigned long long* used;  // [3]: ints used, doubles used, update rows used
   unsigned long long icap, dcap;
   int64_t* u_off;   // [nn] into the solve's update-vector pool (units of rows)
-  int* err;         // [4]: [0] overflow flag, [1] node of first error,
+  int* err;         // [4]: [0] failure bits (1: a pool ran out, 2: a front
+                    // above its launch's on-chip size), [1] node of first error,
                     // [2] completion ticket of the trailing-update launch
   int* inertia;     // [2] pos, neg
   double* flops;    // [kWork] executed flops: [0] all fronts, [1] big panels,
@@ -208,12 +209,14 @@ struct FactorParams {
 constexpr int kSmemFrontMax = 144;
 constexpr int kFactorThreads = 256;
 
+// fmax: the largest front the launch may meet on chip (its shared memory is
+// sized for it); fronts above kSmemFrontMax go to the big-front path
 void launch_factor_level(const DevPlan& p, const DevState& s,
-                         const int* level_nodes, int count,
+                         const int* level_nodes, int count, int fmax,
                          const FactorParams& prm, cudaStream_t stream,
                          const double* vals, const double* diag);
 cudaError_t configure_factor_kernels();
-size_t factor_smem_bytes();
+size_t factor_smem_bytes(int f);
 
 // Big-front pipeline for one level (see big.cu).
 struct BigLevelInfo {
