@@ -303,10 +303,30 @@ __device__ int phase_d_prepare(const DevState& s, BigFront* B, int* done, int* m
     const int nd = xi[kIDcnt];
     const int k = B->k;
     int ncand = B->ncand;
+    // The next panel's first test needs the exact maximum below the block
+    // (rows from k + kBlk on) of every block column. An interchange of rows
+    // a (in the block) and b (below it) takes row b's entry out of a
+    // column's rows below and puts the entry of row a in: thread g < kBlk
+    // follows column k + g, which is formed again afterwards only if the
+    // entry taken out may have been its maximum, or if it is a or b.
+    const int ct = k + g;
+    const bool trk = g < kBlk && ct < f;
+    bool stale = false;
+    double mx = trk ? X[kXNext + g] : 0.0;
     for (int q = 0; q < nd; q++) {
       const int a = xi[kIDpos + q];
       const int b = ncand - 1;
       if (a < b) {
+        if (trk) {
+          if (ct == a || ct == b) {
+            stale = true;
+          } else if (b >= k + kBlk) {
+            const double out = fabs(fsym(F, f, b, ct)), in = fabs(fsym(F, f, a, ct));
+            if (out >= mx) stale = true;
+            mx = fmax(mx, in);
+          }
+        }
+        group_sync<NT>();  // those reads before the interchange
         // the pairs of a symmetric interchange are distinct entries: eight
         // passes of the group load theirs before any is stored back
         constexpr int kU = 8;
@@ -359,38 +379,30 @@ __device__ int phase_d_prepare(const DevState& s, BigFront* B, int* done, int* m
       ncand--;
       group_sync<NT>();
     }
-    // The next panel's first test needs the exact maximum below the block
-    // of the column it tests. The interchanges exchanged rows inside the
-    // block's positions with rows below them, so the maxima are formed
-    // again from the columns (rows from k + kBlk on, contiguous in the lower
-    // triangle): every position of the block when a CTA applies the delays,
-    // the positions that received another candidate when a warp does.
-    if constexpr (NT > 32) {
-      const int lane = g & 31, wq = g >> 5;
-      for (int c = k + wq; c < k + kBlk && c < f; c += NT / 32) {
-        const double* col = F + (size_t)f * c;
-        double m = 0.0;
-        for (int i = k + kBlk + lane; i < f; i += 32) m = fmax(m, fabs(col[i]));
-        m = warp_max(m);
-        if (lane == 0) X[kXNext + (c - k)] = m;
+    // the block columns whose maximum below may have changed, formed again
+    unsigned redo;
+    if constexpr (NT == 32) {
+      redo = __ballot_sync(0xffffffffu, trk && stale);
+    } else {
+      __shared__ unsigned redo_sh;
+      if (g < 32) {
+        const unsigned m = __ballot_sync(0xffffffffu, trk && stale);
+        if (g == 0) redo_sh = m;
       }
       group_sync<NT>();
-    } else {
-      for (int q = 0; q < nd; q++) {
-        const int a = xi[kIDpos + q];
-        const int b = B->ncand - 1 - q;
-        for (int h = 0; h < 2; h++) {
-          const int c = h ? b : a;
-          if (c - k >= kBlk || (h && b <= a)) continue;
-          const double* col = F + (size_t)f * c;
-          double m = 0.0;
-          for (int i = k + kBlk + g; i < f; i += NT) m = fmax(m, fabs(col[i]));
-          m = warp_max(m);
-          if (g == 0) X[kXNext + (c - k)] = m;
-          group_sync<NT>();
-        }
-      }
+      redo = redo_sh;
     }
+    if (trk && !stale) X[kXNext + g] = mx;
+    const int lane = g & 31, wq = g >> 5;
+    for (int i = wq; i < kBlk; i += NT / 32) {
+      if (!((redo >> i) & 1u)) continue;
+      const double* col = F + (size_t)f * (k + i);
+      double m = 0.0;
+      for (int r = k + kBlk + lane; r < f; r += 32) m = fmax(m, fabs(col[r]));
+      m = warp_max(m);
+      if (lane == 0) X[kXNext + i] = m;
+    }
+    group_sync<NT>();
     if (g == 0) {
       B->ncand = ncand;
       B->pending = 0;
