@@ -9,42 +9,51 @@
 // parent. Once the candidates are arranged so that nearly every one passes
 // where it stands (pivot-order reuse), that sequence of column-wide tests is
 // what costs time, not arithmetic. Here a panel of up to 32 candidates of
-// every front of a tree level is decided in four data-parallel phases:
+// every front of a tree level is decided in data-parallel phases:
 //
-//   D. (one warp per front) Delays left by the previous panel are applied
-//      with the reference's symmetric interchange (symm_swap,
-//      sparse_ldl.h:1270-1292). Then the 32 x 32 diagonal block is factored
-//      in shared memory with the reference's tests (lane r owns block row
-//      r). A test's column maximum joins the block's rows with, for the
-//      panel's first pivot, the column's maximum below the block that the
-//      previous panel's trailing update left behind. A pair that formed a
-//      2x2 pivot in the pivot record is tried as that 2x2 first. A
-//      candidate that fails is rotated behind the block's candidates.
+//   D. Delays left by the previous panel are applied with the reference's
+//      symmetric interchange (symm_swap, sparse_ldl.h:1270-1292), by the
+//      whole CTA when the level has no more fronts than CTAs, else by one
+//      warp per front; the next block's column maxima below follow the
+//      interchanges. Then one warp factors the 32 x 32 diagonal block with
+//      the reference's tests (lane r owns block row r), left-looking: a
+//      column is formed from the loaded block and the pivots taken when a
+//      test reads it. A test's column maximum joins the block's rows with,
+//      for the panel's first pivot, the column's exact maximum below the
+//      block that the previous panel's trailing update left behind. A pair
+//      that formed a 2x2 pivot in the pivot record is tried as that 2x2
+//      first. A candidate that fails is rotated behind the block's
+//      candidates.
 //   R. (row chunks) Every row below the block forms its entries of the
 //      pivot columns, W = F21 L11^-T (the values the reference's tests see),
 //      stores them for the trailing update, and the column maxima over all
-//      rows below are reduced.
-//   A. (row chunks) The reference's tests are evaluated exactly, with the
-//      column maxima over the whole front; the pivots before the first
-//      failure are accepted and written as L (D on the diagonal, 2x2 blocks
-//      with d21 below it, as the reference stores them). The first rejected
-//      pivot, and the candidates that failed in the block while only
-//      accepted pivots preceded them, are delayed at the next phase D.
-//   U. (64 x 64 tiles) The trailing matrix gets the rank-kw update of the
-//      accepted pivots.
+//      rows below are reduced. The front's last chunk to finish runs the
+//      reference's tests exactly, with the column maxima over the whole
+//      front, and records how many leading pivots pass.
+//   A+U. The row chunks write L for the passing pivots (D on the diagonal,
+//      2x2 blocks with d21 below it, as the reference stores them) and the
+//      first of them commits the panel; beside them, 64 x 64 tiles give the
+//      trailing matrix the rank-kw update, forming L from W as the commit
+//      does. The first rejected pivot, and the candidates that failed in
+//      the block while only accepted pivots preceded them, are delayed at
+//      the next phase D. (In the mixed-precision mode the commit and the
+//      update are separate phases: the tensor-core tiles read L from the
+//      front.)
 //
 // Every accepted pivot therefore satisfies the reference's threshold test
 // against its whole column, so the factorization has the reference's
 // stability bound (|L| <= 1/ustab for 1x1 pivots) and, by Sylvester's law,
 // its inertia; only the order in which candidates are tried differs (a
-// candidate's 2x2 partner is searched within its panel's block).
+// candidate's 2x2 partner is searched within its panel's block). A root
+// cannot delay: the candidates its tests leave are finished by the chained
+// panels (Bunch-Kaufman) after the level's launch.
 //
 // The phases run in one cooperative launch per level, separated by grid-wide
-// barriers: a panel step costs four barriers instead of five kernel
-// launches. Every CTA runs the same phases and barriers; the loop ends for
-// all of them on a count that the barrier makes visible to all, or at a cap
-// that the progress of every step guarantees not to reach (each step of an
-// active front accepts a pivot or delays a candidate).
+// barriers: three per panel step. Every CTA runs the same phases and
+// barriers; the loop ends for all of them on a count that the barrier makes
+// visible to all, or at a cap that the progress of every step guarantees
+// not to reach (each step of an active front accepts a pivot or delays a
+// candidate).
 //
 // The front stays in HBM in logical order between steps (column-major,
 // lower triangle, the layout big_chain.cu and big_update_kernel use). A
