@@ -88,10 +88,25 @@ __device__ void block_reduce(BlockRed& r, double& bv, int& bi, double& cm) {
 
 // ---------------------------------------------------------------- assembly
 
-// Assembly of every big front of a level in one launch: a front per
-// cluster of CL CTAs (CL = 1: a front per CTA). The cluster zeroes the
-// front's lower triangle with Sigma already on the own variables' diagonal,
-// adds the CSR entries of its pivot columns, then extend-adds its children's
+// Zero the lower triangle of every big front of a level: independent of
+// the assembly order, so every SM takes part (a CTA per eight columns).
+__global__ void big_zero_kernel(DevState s, const int* __restrict__ list) {
+  const BigFront& B = s.big[list[blockIdx.x]];
+  double* F = s.dpool + B.doff;
+  const int f = B.f;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  for (int j = blockIdx.y * nw + warp; j < f; j += gridDim.y * nw) {
+    double* col = F + (size_t)f * j;
+    for (int i = j + lane; i < f; i += 32) col[i] = 0.0;
+  }
+}
+
+// Assembly of every big front of a level in one launch, after
+// big_zero_kernel: a front per cluster of CL CTAs (CL = 1: a front per CTA).
+// The cluster writes Sigma on the own variables' diagonal, adds the CSR
+// entries of its pivot columns, then extend-adds its children's
 // contribution blocks one child after another, with a cluster barrier
 // between the steps. Each entry therefore receives its terms in the order
 // diag, CSR value, children in child order; since the front starts at zero
@@ -120,12 +135,10 @@ __global__ void __launch_bounds__(256) big_assemble_kernel(DevPlan p, DevState s
   const int warp = threadIdx.x >> 5;
   constexpr int kW = 8;  // warps per CTA
   const int v0 = p.var_ptr[node];
-  // zero, with the diagonal of the own variables set to Sigma
-  for (int j = rank * kW + warp; j < f; j += CL * kW) {
-    double* col = F + (size_t)f * j;
-    const double dj = (diag && j < ns) ? diag[p.node_to_var[v0 + j]] : 0.0;
-    for (int i = j + lane; i < f; i += 32) col[i] = (i == j) ? dj : 0.0;
-  }
+  // Sigma on the diagonal of the own variables (the front is zero)
+  if (diag)
+    for (int j = rank * blockDim.x + threadIdx.x; j < ns; j += CL * blockDim.x)
+      F[j + (size_t)f * j] = diag[p.node_to_var[v0 + j]];
   // a-posteriori panels: no column maxima for the first panel yet
   if (B.app && rank == 0 && threadIdx.x < kBigPanelMax)
     s.dpool[B.xoff + kAppNextColmax + threadIdx.x] = 0.0;
@@ -809,18 +822,21 @@ cudaError_t launch_assemble_cl(const DevPlan& p, const DevState& s, const int* l
 // One launch for the level's fronts in `list`: a CTA per front when they
 // fill the GPU, otherwise a cluster of 4 or 16 CTAs per front.
 cudaError_t assemble_big(const DevPlan& p, const DevState& s, const int* list, int nl,
-                         const double* vals, const double* diag, cudaStream_t stream,
+                         int max_f, const double* vals, const double* diag, cudaStream_t stream,
                          Prof& prof) {
   if (nl <= 0) return cudaSuccess;
   prof.begin(stream);
-  cudaError_t e;
+  big_zero_kernel<<<dim3(nl, std::max(1, std::min(256, (max_f + 7) / 8))), 256, 0, stream>>>(s,
+                                                                                        list);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
   if (nl >= 148)
     e = launch_assemble_cl<1>(p, s, list, nl, vals, diag, stream);
   else if (nl >= 37)
     e = launch_assemble_cl<4>(p, s, list, nl, vals, diag, stream);
   else
     e = launch_assemble_cl<16>(p, s, list, nl, vals, diag, stream);
-  prof.end(kPhBigAsm, stream, 1);
+  prof.end(kPhBigAsm, stream, 2);
   return e;
 }
 
@@ -870,7 +886,7 @@ cudaError_t app_level(const DevPlan& p, const DevState& s, const BigLevelInfo& i
                       const double* diag, cudaStream_t stream, Prof& prof) {
   const int nl = info.count_app;
   const int* list6 = s.class_list + (size_t)6 * p.num_nodes;
-  cudaError_t e = assemble_big(p, s, list6, nl, vals, diag, stream, prof);
+  cudaError_t e = assemble_big(p, s, list6, nl, info.max_f_app, vals, diag, stream, prof);
   if (e != cudaSuccess) return e;
   prof.begin(stream);
   int* list7 = s.class_list + (size_t)7 * p.num_nodes;
@@ -936,7 +952,8 @@ cudaError_t launch_big_level(const DevPlan& p, const DevState& s, const BigLevel
   // in global memory
   const int* list5 = s.class_list + (size_t)5 * p.num_nodes;
   {
-    cudaError_t e = assemble_big(p, s, list5, info.count_large, vals, diag, stream, prof);
+    cudaError_t e =
+        assemble_big(p, s, list5, info.count_large, info.max_f_large, vals, diag, stream, prof);
     if (e != cudaSuccess) return e;
     e = run_big_panels(s, prm, list5, info.count_large, info.max_f_large, info.max_fs_large,
                        stream, prof);
