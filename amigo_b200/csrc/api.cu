@@ -122,6 +122,10 @@ struct b200ldl_handle {
   // a level whose fronts cannot exceed the shared-memory limit, whatever the
   // delays, needs no big-front launch (and no host read-back)
   std::vector<char> level_may_big;
+  // per level: whether the host prepares big fronts (a device sync per such
+  // level): the levels that had one in the last factorization, the levels
+  // whose bound allows one until then
+  std::vector<char> level_big;
   std::vector<int> level_fbound;  // per level: bound on its on-chip fronts (shared memory sizing)
   // per level: the on-chip front size its small-front launch is given, the
   // last factorization's largest front plus slack (the bound until then)
@@ -304,6 +308,7 @@ void build_plan(b200ldl_t h, const int* rowp, const int* cols) {
           std::max(h->level_fbound[level[k]], (int)std::min<long long>(fb, kSmemFrontMax));
     }
     h->level_fcap = h->level_fbound;
+    h->level_big = h->level_may_big;
   }
   h->h_ns = ns;
   h->h_nc = nc;
@@ -557,14 +562,14 @@ void run_factor_once(b200ldl_t h, const double* vals, const double* diag, bool m
     for (int l = 0; l < h->num_levels; l++) {
       const int b = h->level_ptr[l];
       const int cnt = h->level_ptr[l + 1] - b;
-      if (h->level_may_big[l])
+      if (h->level_big[l])
         CK(cudaMemsetAsync(h->d_big_meta.ptr, 0, kBigMeta * sizeof(int), h->stream));
       h->prof.begin(h->stream);
-      launch_factor_level(h->plan, h->st, h->d_level_nodes.ptr + b, cnt, h->level_fcap[l], prm,
-                          h->stream, vals, diag);
+      launch_factor_level(h->plan, h->st, h->d_level_nodes.ptr + b, cnt, h->level_fcap[l],
+                          h->level_big[l], prm, h->stream, vals, diag);
       h->prof.end(kPhFront, h->stream, 1);
       CK(cudaGetLastError());
-      if (!h->level_may_big[l]) continue;
+      if (!h->level_big[l]) continue;
       int meta[kBigMeta];
       CK(cudaMemcpyAsync(meta, h->d_big_meta.ptr, kBigMeta * sizeof(int), cudaMemcpyDeviceToHost,
                          h->stream));
@@ -624,8 +629,14 @@ void run_factor_once(b200ldl_t h, const double* vals, const double* diag, bool m
         const int fm = h->level_fmax[l];
         h->level_fcap[l] = std::min(h->level_fbound[l],
                                     std::min(kSmemFrontMax, fm + std::max(8, fm / 4)));
+        h->level_big[l] = fm > kSmemFrontMax ? 1 : 0;
       }
       return;
+    }
+    if (err[0] & 4) {
+      // a front went big in a level not prepared for one: every level whose
+      // bound allows one is prepared
+      h->level_big = h->level_may_big;
     }
     if (err[0] & 2) {
       // a front outgrew its launch's on-chip size: every level gets its

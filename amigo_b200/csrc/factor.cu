@@ -121,7 +121,7 @@ enum : int { kDelay = 0, kOne = 1, kTwo = 2, kNeedRow = 3, kZero = 4 };
 __global__ void __launch_bounds__(kFactorThreads)
     factor_level_kernel(DevPlan p, DevState s, const int* __restrict__ nodes,
                         const double* __restrict__ vals, const double* __restrict__ diag,
-                        FactorParams prm, int fcap) {
+                        FactorParams prm, int fcap, int allow_big) {
   extern __shared__ __align__(16) double smem[];
   __shared__ Reduce red;
   __shared__ int sh_fail;
@@ -151,6 +151,13 @@ __global__ void __launch_bounds__(kFactorThreads)
     // the factorization, which the host repeats with room for every front
     if (!big && f > fcap) {
       atomicOr(s.err, 2);
+      atomicCAS(s.err + 1, -1, node);
+      sh_fail = 1;
+    }
+    // a big front in a level the host does not prepare big fronts for stops
+    // the factorization too; the host repeats it with every level prepared
+    if (big && !allow_big) {
+      atomicOr(s.err, 4);
       atomicCAS(s.err + 1, -1, node);
       sh_fail = 1;
     }
@@ -673,11 +680,11 @@ size_t factor_smem_bytes(int f) {
 }
 
 void launch_factor_level(const DevPlan& p, const DevState& s, const int* level_nodes,
-                         int count, int fmax, const FactorParams& prm, cudaStream_t stream,
-                         const double* vals, const double* diag) {
+                         int count, int fmax, int allow_big, const FactorParams& prm,
+                         cudaStream_t stream, const double* vals, const double* diag) {
   if (count <= 0) return;
   factor_level_kernel<<<count, kFactorThreads, factor_smem_bytes(fmax), stream>>>(
-      p, s, level_nodes, vals, diag, prm, fmax);
+      p, s, level_nodes, vals, diag, prm, fmax, allow_big);
 }
 
 cudaError_t configure_factor_kernels() {

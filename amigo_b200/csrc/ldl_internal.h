@@ -147,7 +147,8 @@ struct DevState {
   unsigned long long icap, dcap;
   int64_t* u_off;   // [nn] into the solve's update-vector pool (units of rows)
   int* err;         // [4]: [0] failure bits (1: a pool ran out, 2: a front
-                    // above its launch's on-chip size), [1] node of first error,
+                    // above its launch's on-chip size, 4: a big front in a
+                    // level not prepared for one), [1] node of first error,
                     // [2] completion ticket of the trailing-update launch
   int* inertia;     // [2] pos, neg
   double* flops;    // [kWork] executed flops: [0] all fronts, [1] big panels,
@@ -210,9 +211,11 @@ constexpr int kSmemFrontMax = 144;
 constexpr int kFactorThreads = 256;
 
 // fmax: the largest front the launch may meet on chip (its shared memory is
-// sized for it); fronts above kSmemFrontMax go to the big-front path
+// sized for it); fronts above kSmemFrontMax go to the big-front path, which
+// the host prepares for the level only with allow_big (else such a front
+// stops the factorization with failure bit 4)
 void launch_factor_level(const DevPlan& p, const DevState& s,
-                         const int* level_nodes, int count, int fmax,
+                         const int* level_nodes, int count, int fmax, int allow_big,
                          const FactorParams& prm, cudaStream_t stream,
                          const double* vals, const double* diag);
 cudaError_t configure_factor_kernels();
