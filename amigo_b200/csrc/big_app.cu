@@ -139,6 +139,18 @@ __device__ __forceinline__ double warp_max(double v) {
   return __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
 }
 
+// The L entries (l0, l1) of a row whose W entries are (a, b) under the 2x2
+// pivot d = (d11, d21, d22): (a, b) D^-1, with explicit fused multiply-adds so
+// that every kernel that forms them gets the same values.
+__device__ __forceinline__ void l_2x2(const double* d, double a, double b, double& l0,
+                                      double& l1) {
+  const double d11 = d[0], d21 = d[1], d22 = d[2];
+  const double di = 1.0 / (d11 * d22 - d21 * d21);
+  const double i00 = d22 * di, i01 = -d21 * di, i11 = d11 * di;
+  l0 = fma(a, i00, b * i01);
+  l1 = fma(a, i01, b * i11);
+}
+
 // ------------------------------------------------------------- shared memory
 
 struct WarpDiag {  // phase D, one per warp
@@ -614,11 +626,13 @@ __device__ int phase_d_block(const DevState& s, const FactorParams& prm, BigFron
     } else {
       const double d11 = __shfl_sync(kFull, p1, t), d21 = __shfl_sync(kFull, p1, t + 1),
                    d22 = __shfl_sync(kFull, p2, t + 1);
-      const double di = 1.0 / (d11 * d22 - d21 * d21);
-      const double i00 = d22 * di, i01 = -d21 * di, i11 = d11 * di;
+      // the expressions of the commit and of the update tiles (l_2x2)
+      const double dv[3] = {d11, d21, d22};
+      double l0, l1;
+      l_2x2(dv, p1, p2, l0, l1);
       if (lane > t + 1 && lane < nbk) {
-        w.Lb[lane][t] = p1 * i00 + p2 * i01;
-        w.Lb[lane][t + 1] = p1 * i01 + p2 * i11;
+        w.Lb[lane][t] = l0;
+        w.Lb[lane][t + 1] = l1;
       }
       if (lane == 0) {
         w.kind[t] = 2;
@@ -794,17 +808,6 @@ __device__ void phase_r_item(const DevState& s, const FactorParams& prm, const B
 
 // ---------------------------------------------------------------- phase A
 
-// The L entries (l0, l1) of a row whose W entries are (a, b) under the 2x2
-// pivot d = (d11, d21, d22): (a, b) D^-1, with explicit fused multiply-adds so
-// that every kernel that forms them gets the same values.
-__device__ __forceinline__ void l_2x2(const double* d, double a, double b, double& l0,
-                                      double& l1) {
-  const double d11 = d[0], d21 = d[1], d22 = d[2];
-  const double di = 1.0 / (d11 * d22 - d21 * d21);
-  const double i00 = d22 * di, i01 = -d21 * di, i11 = d11 * di;
-  l0 = fma(a, i00, b * i01);
-  l1 = fma(a, i01, b * i11);
-}
 
 __device__ void phase_a_item(const DevState& s, const FactorParams& prm, BigFront* B, int chunk,
                              RowsSm& sm) {
