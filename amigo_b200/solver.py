@@ -59,14 +59,40 @@ class B200LdlSolver(LinearSolver):
     """AmigoSolver's contract on the GPU: symbolic analysis once for the
     Hessian's pattern (AMD, ustab 0.01, pivot_tol 1e-14), numeric
     factorization and inertia on every ``factor``, solve on the stored
-    factor."""
+    factor.
+
+    ``reuse_pivot_order=True`` makes the factorizations after the first one
+    test each candidate in the front that accepted it in a recent
+    factorization (SparseLDL.reuse_pivot_order). The structure is re-planned
+    before the second factorization, and again before the factorization that
+    follows one which delayed more than ``refresh_delays * n`` candidates
+    (the iterates moved away from the record). Every threshold test still
+    applies, so the inertia is the same; the values differ in rounding.
+    Off by default: every factorization then replays the reference's pivot
+    sequence."""
 
     def __init__(self, options=None, state=None, hessian=None, ustab: float = 0.01,
-                 pivot_tol: float = 1e-14, order=OrderingType.DEFAULT):
+                 pivot_tol: float = 1e-14, order=OrderingType.DEFAULT,
+                 reuse_pivot_order: bool = False, refresh_delays: float = 0.01):
         self.options = options
         self.hessian = hessian if hessian is not None else state.hessian
         self.ldl = SparseLDL(self.hessian, SolverType.LDL, ustab=ustab, pivot_tol=pivot_tol,
                              order=order)
+        self.reuse_pivot_order = bool(reuse_pivot_order)
+        self.refresh_delays = float(refresh_delays)
+        self._replan = False  # re-plan from the last record before the next factorization
+        self._planned = False
+
+    def _before_factor(self):
+        if self._replan:
+            self.ldl.reuse_pivot_order()  # drops the last factor: only right before factoring
+            self._replan = False
+            self._planned = True
+
+    def _after_factor(self):
+        if self.reuse_pivot_order:
+            delayed = self.ldl.stats()["delayed"]
+            self._replan = (not self._planned) or delayed > self.refresh_delays * self.ldl.n
 
     def factor(self, hessian, diagonal):
         if hessian is not self.hessian and hessian != self.hessian:
@@ -77,9 +103,11 @@ class B200LdlSolver(LinearSolver):
             diagonal.copy_device_to_host()
         if hasattr(self.hessian, "copy_data_device_to_host"):
             self.hessian.copy_data_device_to_host()
+        self._before_factor()
         flag = self.ldl.factor(diagonal)
         if flag != 0:
             raise RuntimeError(f"B200LdlSolver factorization failed with flag = {flag}")
+        self._after_factor()
         return flag
 
     def solve(self, b, x):
@@ -129,4 +157,7 @@ class B200LdlSolver(LinearSolver):
     def factor_perturbed(self, delta_x, delta_c):
         """One attempt on the loaded system; returns (npos, nneg)."""
         vals, diag = self._dev
-        return self.ldl.factor_perturbed(delta_x, delta_c, vals, diag)
+        self._before_factor()
+        out = self.ldl.factor_perturbed(delta_x, delta_c, vals, diag)
+        self._after_factor()
+        return out

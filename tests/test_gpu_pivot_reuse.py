@@ -3,6 +3,8 @@ own pivot record, factored again on the device. Inertia must equal the
 compiled reference's and the backward error stay at the FP64 level, both for
 the values the record came from and for other values of the same pattern."""
 
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -66,3 +68,32 @@ def test_optimal_control_and_batch_reuse():
     for q, xs, inert in zip(systems, batch.split(xb), batch.system_inertia()):
         assert tuple(int(v) for v in inert) == q.expected_inertia
         assert backward_error(q, xs.reshape(-1, 1), q.rhs[:, :1]) <= BERR_TOL
+
+
+def test_plugin_reuses_and_refreshes_the_pivot_order():
+    """B200LdlSolver with reuse_pivot_order: the second factorization runs on
+    the structure re-planned from the first, and with refresh_delays = 0
+    every factorization that delays a candidate re-plans the next one from
+    its own record (a record taken on a re-planned structure). Inertia as
+    the compiled reference gives it and FP64-level backward errors on the
+    benchmark values, a neighbouring iterate's values, and back."""
+    from amigo_b200.solver import B200LdlSolver
+    from tests.test_gpu_configs import _perturbed_values
+
+    s = plane_stress_kkt(48)
+    mat = CSRMat(s.n, s.n, s.rowp, s.cols, s.vals.copy())
+    solver = B200LdlSolver(hessian=mat, order=OrderingType.AMD, reuse_pivot_order=True,
+                           refresh_delays=0.0)
+    pv, pd = _perturbed_values(s)
+    b = s.rhs[:, 0].copy()
+    for vals, diag in ((s.vals, s.diag), (pv, pd), (s.vals, s.diag), (pv, pd)):
+        mat.vals[:] = vals
+        solver.factor(mat, diag)
+        r = ref.RefLDL(s.rowp, s.cols, order=ref.ORDER_AMD)
+        r.factor(vals, diag)
+        assert tuple(solver.get_inertia()) == tuple(r.inertia())
+        x = np.empty(s.n)
+        solver.solve(b, x)
+        sys_ = dataclasses.replace(s, vals=np.asarray(vals), diag=np.asarray(diag))
+        assert backward_error(sys_, x.reshape(-1, 1), b.reshape(-1, 1)) <= 1e-12
+    assert solver._planned
